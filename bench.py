@@ -1,0 +1,341 @@
+"""Benchmark of the virtual-PE one-sided path on B200.
+
+Headline (one JSON line on rank 0): batched put/get throughput of the C4
+workload -- 64 virtual PEs x 64 MiB heap, 100,000 requests per batch with
+log-normal sizes (median 2 KiB, sigma 1.5, 4 B..4 MiB), put 45% / get 45% /
+signal 10%, uniform PE pairs, disjoint destinations -- in GB/s counting 2
+bytes per payload byte (read + write), with L2 flushed between steps.
+Beside it: the per-call path on the same batch, the end-to-end call with
+host-resident requests, the C2 all-to-all bulk throughput, the C1 ping-pong
+round trip and the device barrier latency, the roofline of the batch's exec
+kernel and the CPU baseline (forked processes + memcpy + process-shared
+barrier, the stand-in for the reference's MPI host path).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "df-nvshmem-prototype_b200", "python"))
+sys.path.insert(0, ROOT)
+
+METRIC = "batched put/get GB/s (% HBM peak) vs per-call path; p50 wait/barrier ns; 1 B200"
+UNIT = "GB/s"
+C4 = dict(seed=4, n=100_000, npes=64, heap=64 << 20)
+WORKLOAD = ("C4 batched uneven traffic: 64 virtual PEs x 64 MiB heap, 100,000 put/get/signal "
+            "requests per batch, log-normal sizes median 2 KiB sigma 1.5 clipped 4 B..4 MiB, "
+            "put 45%/get 45%/signal 10%, uniform PE pairs, disjoint 16-B-aligned destinations, seed 4")
+TUNED = os.path.join(ROOT, "df-nvshmem-prototype_b200", "tuned", "batch_c4.json")
+NCU_SUMMARY = os.path.join(ROOT, "profiles", "batch_exec_c4.json")
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev: int):
+        self.dev = dev
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(self.dev)], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]})
+        load = sorted(sm)[len(sm) // 2:] if sm else []
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------ distributed
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def dist_init(world):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group("nccl" if os.environ.get("BENCH_BACKEND", "nccl") == "nccl" else "gloo",
+                            timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def reduce_max(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# ------------------------------------------------------------ CPU baseline
+def cpu_baseline(reqs, npes, heap, max_seconds=12.0):
+    from oracle import model as om  # the checker package; only this leg runs it
+    if not os.path.exists(om.HOST_BENCH):
+        om.build()
+    with tempfile.NamedTemporaryFile(suffix=".req", delete=False) as f:
+        f.write(reqs.tobytes())
+        path = f.name
+    try:
+        out = subprocess.run([om.HOST_BENCH, "batch", path, str(npes), str(heap), "1000000", str(max_seconds), "44"],
+                             capture_output=True, text=True, timeout=600, check=True).stdout
+    finally:
+        os.unlink(path)
+    r = json.loads(out.strip().splitlines()[-1])
+    return {"value": round(r["gbs"], 3), "unit": UNIT, "cores": r["cores"], "kind": "port",
+            "ms_per_step": 1e3 * r["seconds_per_rep"], "reps": r["reps"],
+            "sample": f"the full {r['requests']}-request batch, {r['npes']} forked ranks, {r['reps']} reps "
+                      f"within {max_seconds:.0f} s (host has {r['host_cores']} cores)",
+            "heap_checksum": r["heap_checksum"]}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the CPU host path on this box's cores (rank 0 only)."""
+    if rank != 0:
+        return
+    import numpy as np  # noqa: F401
+    from nvshmem_b200.traffic import c4_batch
+    reqs = c4_batch(**C4)
+    t0 = time.time()
+    cb = cpu_baseline(reqs, C4["npes"], C4["heap"], max_seconds=max(5.0, 2.0 * args.steps))
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": cb["reps"],
+            "warmup": 1, "ms_per_step": round(cb["ms_per_step"], 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": WORKLOAD, "parallelism": "one OS process per PE"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": round(time.time() - t0, 1)}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------- GPU arm
+def l2_flusher():
+    import torch
+    buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def flush():
+        buf.fill_(1)
+        torch.cuda.synchronize()
+    return flush
+
+
+def load_tuned():
+    if os.path.exists(TUNED):
+        with open(TUNED) as f:
+            return json.load(f).get("best")
+    return None
+
+
+def run_gpu(args, rank, world, local):
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    from nvshmem_b200 import MODE_BLOCK, MODE_BULK, MODE_THREAD, MODE_WARP, REQ_PUT, DT_FLOAT, Shmem, requests_bytes
+    from nvshmem_b200.traffic import c4_batch
+
+    dist = dist_init(world)
+    peak, peak_kind = measured_peak()
+    flush = l2_flusher()
+    reqs = c4_batch(**C4)
+    alg = requests_bytes(reqs)
+    payload = int(reqs["bytes"].sum())
+    out = {}
+    sampler = ClockSampler(local)
+    with sampler:
+        with Shmem(C4["npes"], C4["heap"]) as sh:
+            for pe in range(C4["npes"]):
+                sh.fill_random(pe, 0, C4["heap"], 44)
+            with sh.batch(len(reqs), payload, 256) as b:
+                tuned = load_tuned()
+                if tuned:
+                    b.set_config(tuned)
+                b.upload(reqs)
+                for _ in range(args.warmup):
+                    flush()
+                    b.execute(1)
+                # device-resident batches: K steps, L2 flushed between steps
+                torch.cuda.synchronize()
+                barrier(dist)
+                step_ms, exec_ms = [], []
+                for _ in range(args.steps):
+                    flush()
+                    step_ms.append(b.execute(1))
+                    exec_ms.append(b.stats()[2])
+                torch.cuda.synchronize()
+                barrier(dist)
+                t_batch = reduce_max(dist, sum(step_ms) / 1e3)
+                chunks = b.stats()[0]
+                # per-call path on the same batch (one thread per request)
+                pc = {}
+                for mode, name in ((MODE_THREAD, "thread"), (MODE_WARP, "warp")):
+                    flush()
+                    b.percall(mode, 1)
+                    ts = []
+                    for _ in range(max(1, args.steps // 5)):
+                        flush()
+                        ts.append(b.percall(mode, 1))
+                    pc[name] = alg / (statistics.median(ts) / 1e3) / 1e9
+                # end to end: host-resident requests each step
+                hb = b.host_buffer()
+                hb[:len(reqs)] = reqs
+                for _ in range(args.warmup):
+                    flush()
+                    b.submit(hb, len(reqs))
+                barrier(dist)
+                e2e_ms = []
+                for _ in range(args.steps):
+                    flush()
+                    st, ms = b.submit(hb, len(reqs))
+                    assert st == 0, f"batch status {st}"
+                    e2e_ms.append(ms)
+                barrier(dist)
+                t_e2e = reduce_max(dist, sum(e2e_ms) / 1e3)
+                cfg_used = b.config()
+            assert sh.status() == 0
+            checks = [sh.checksum(pe, 0, C4["heap"]) for pe in range(C4["npes"])]
+        # latency metrics: ping-pong (C1) and device barrier (8 PEs)
+        with Shmem(2, 8 << 20) as sh:
+            flag = sh.alloc(4)
+            ns, _ = sh.pingpong(flag, 0, 0, 10000, 20)
+            out["pingpong_rtt_ns"] = {"p50": round(float(np.percentile(ns, 50)), 1),
+                                      "p99": round(float(np.percentile(ns, 99)), 1), "iters": 10000}
+        with Shmem(8, 1 << 20) as sh:
+            bar = {}
+            for ctas in (1, 16):
+                ns, _ = sh.barrier_latency(ctas, 10000)
+                bar[f"{ctas}_cta_per_pe"] = {"p50": round(float(np.percentile(ns, 50)), 1),
+                                             "p99": round(float(np.percentile(ns, 99)), 1)}
+            out["barrier_ns"] = bar
+            out["offload_barrier_us_per_call"] = round(sh.offload_barrier(1000), 3)
+        # C2 bulk all-to-all: 8 PEs, 1 MiB and 16 MiB messages, rotating sets > 2x L2
+        a2a = {}
+        for nbytes in (1 << 20, 16 << 20):
+            nsets = max(2, (512 << 20) // (2 * 8 * 8 * nbytes) + 1)
+            heap = 2 * 8 * nbytes * nsets
+            with Shmem(8, heap) as sh:
+                for pe in range(8):
+                    sh.fill_random(pe, 0, heap, 1)
+                rounds = 4 * nsets
+                for mode, name in ((MODE_BLOCK, "block"), (MODE_BULK, "bulk")):
+                    ctas = 18 if name == "block" else 18
+                    sh.alltoall(REQ_PUT, DT_FLOAT, 0, 8 * nbytes, nbytes, rounds=nsets, nsets=nsets,
+                                set_stride=16 * nbytes, mode=mode, ctas_per_pe=ctas)
+                    ms = sh.alltoall(REQ_PUT, DT_FLOAT, 0, 8 * nbytes, nbytes, rounds=rounds, nsets=nsets,
+                                     set_stride=16 * nbytes, mode=mode, ctas_per_pe=ctas)
+                    gbs = 2 * 8 * 7 * nbytes * rounds / (ms / 1e3) / 1e9
+                    a2a[f"{nbytes >> 20}MiB_{name}"] = {"GBps": round(gbs, 1), "frac": round(gbs / peak, 3)}
+                assert sh.status() == 0
+        out["alltoall_8pe"] = a2a
+    clocks = sampler.summary()
+
+    value = world * alg * args.steps / t_batch / 1e9
+    e2e = world * alg * args.steps / t_e2e / 1e9
+    exec_avg = statistics.mean(exec_ms) / 1e3
+    achieved = alg / exec_avg / 1e9
+    traffic = None
+    if os.path.exists(NCU_SUMMARY):
+        with open(NCU_SUMMARY) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * t_batch / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "l2": "flushed between steps (256 MiB write)",
+                   "parallelism": f"replicas x{world}", "batch_config": cfg_used,
+                   "alg_bytes_per_step": alg, "chunks": chunks},
+        "frac_of_hbm": round(value / peak, 3),
+        "percall_GBps": {k: round(v, 2) for k, v in pc.items()},
+        "speedup_vs_percall_thread": round(value / pc["thread"], 2),
+        "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(len(reqs) * 32),
+                "d2h_bytes_per_step": 8},
+        "gpu_launches": 2 * args.steps * 2,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 3), "traffic": traffic,
+                     "kernel": "batch_exec_kernel", "peak_kind": peak_kind},
+        "clocks": clocks,
+        "heap_checksum": int(sum(checks) % (1 << 64)),
+    }
+    line.update(out)
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = {k: v for k, v in cpu_baseline(reqs, C4["npes"], C4["heap"]).items()
+                                if k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_gpu(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

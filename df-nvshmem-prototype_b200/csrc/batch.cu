@@ -1,0 +1,480 @@
+// batch.cu -- batched one-sided traffic (nvshmemx_batch.h).
+//
+// A batch runs as a CUDA graph of three nodes on the batch's own stream:
+//   memset   zero the 32-byte control block (chunk count, cursor, status)
+//   plan     one thread per request: validate, translate to arena addresses,
+//            cut into chunks of <= chunk_bytes; a CTA-wide scan plus one
+//            atomicAdd per CTA places each CTA's chunks in the work table
+//            (CTA order is arbitrary, which is fine: requests are disjoint)
+//   exec     persistent grid (SM count x CTAs per SM); each warp claims
+//            `grab` chunks per atomicAdd on the cursor, prefetches the next
+//            claim and the next 32-byte work item while it copies the current
+//            chunk with VB-byte accesses, U in flight per lane.
+// Every chunk is a contiguous copy, so the exec kernel is pure streaming:
+// its roofline is HBM copy bandwidth (2 bytes moved per payload byte).
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "batch.h"
+#include "nvshmemx_batch.h"
+
+namespace nvshm {
+
+struct WorkItem {          // 32 bytes
+  unsigned long long dst;  // absolute destination address
+  unsigned long long src;  // absolute source address (P: the element bits)
+  unsigned int len;        // bytes
+  unsigned int kind;       // kCopy, kSignal, kStore
+  int value;               // SIGNAL value
+  unsigned int pad;
+};
+enum { kCopy = 0, kSignal = 1, kStore = 2 };
+
+struct BatchCtl {  // 32 bytes, zeroed before every execution
+  unsigned long long total_chunks;
+  unsigned long long cursor;
+  int status;
+  int bad_request;
+  unsigned long long pad;
+};
+
+__device__ __forceinline__ void set_status(BatchCtl *ctl, int code, int req) {
+  if (atomicCAS(&ctl->status, 0, code) == 0) ctl->bad_request = req;
+}
+
+// ------------------------------------------------------------------- plan
+__global__ void __launch_bounds__(256) batch_plan_kernel(Cfg c, const nvshmemx_request *__restrict__ reqs, int n,
+                                                         unsigned chunk, WorkItem *__restrict__ items,
+                                                         unsigned long long cap, BatchCtl *ctl) {
+  __shared__ unsigned warp_sums[8];
+  __shared__ unsigned long long block_base;
+  const int i = blockIdx.x * 256 + threadIdx.x;
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  unsigned cnt = 0;
+  WorkItem w;
+  w.dst = w.src = 0;
+  w.len = 0;
+  w.kind = kCopy;
+  w.value = 0;
+  w.pad = 0;
+  if (i < n) {
+    const nvshmemx_request r = reqs[i];
+    const unsigned width = r.dtype == NVSHMEMX_DT_DOUBLE ? 8u : 4u;
+    const bool pe_ok = r.src_pe < c.npes && r.dst_pe < c.npes && r.dtype <= NVSHMEMX_DT_DOUBLE;
+    const unsigned long long dst = (unsigned long long)c.arena + ((unsigned long long)r.dst_pe << c.log2_stride) + r.dst_off;
+    const unsigned long long src = (unsigned long long)c.arena + ((unsigned long long)r.src_pe << c.log2_stride) + r.src_off;
+    switch (r.op) {
+      case NVSHMEMX_REQ_PUT:
+      case NVSHMEMX_REQ_GET:
+      case NVSHMEMX_REQ_G: {
+        const unsigned long long bytes = r.op == NVSHMEMX_REQ_G ? width : r.bytes;
+        if (!pe_ok || r.src_off + bytes > c.slice_bytes || r.dst_off + bytes > c.slice_bytes) {
+          set_status(ctl, NVSHMEMX_ERR_BOUNDS, i);
+          break;
+        }
+        w.dst = dst;
+        w.src = src;
+        w.len = (unsigned)bytes;
+        cnt = bytes ? (unsigned)((bytes + chunk - 1) / chunk) : 0u;
+        break;
+      }
+      case NVSHMEMX_REQ_SIGNAL:
+      case NVSHMEMX_REQ_P: {
+        const unsigned bytes = r.op == NVSHMEMX_REQ_SIGNAL ? 4u : width;
+        if (!pe_ok || r.dst_off + bytes > c.slice_bytes || (r.dst_off & (bytes - 1))) {
+          set_status(ctl, NVSHMEMX_ERR_BOUNDS, i);
+          break;
+        }
+        w.dst = dst;
+        w.src = r.src_off;
+        w.len = bytes;
+        w.kind = r.op == NVSHMEMX_REQ_SIGNAL ? kSignal : kStore;
+        w.value = r.value;
+        cnt = 1;
+        break;
+      }
+      default:
+        set_status(ctl, NVSHMEMX_ERR_INVALID, i);
+    }
+  }
+  // CTA-wide exclusive scan of cnt
+  unsigned incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= (unsigned)o) incl += v;
+  }
+  if (lane == 31) warp_sums[warp] = incl;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned acc = 0;
+    for (int k = 0; k < 8; ++k) {
+      unsigned s = warp_sums[k];
+      warp_sums[k] = acc;
+      acc += s;
+    }
+    block_base = acc ? atomicAdd(&ctl->total_chunks, (unsigned long long)acc) : 0ull;
+    if (acc && block_base + acc > cap) set_status(ctl, NVSHMEMX_ERR_NOMEM, -1);
+  }
+  __syncthreads();
+  if (cnt == 0) return;
+  const unsigned long long first = block_base + warp_sums[warp] + (incl - cnt);
+  if (first + cnt > cap) return;
+  if (cnt == 1) {
+    items[first] = w;
+    return;
+  }
+  for (unsigned k = 0; k < cnt; ++k) {
+    WorkItem p = w;
+    const unsigned long long off = (unsigned long long)k * chunk;
+    p.dst += off;
+    p.src += off;
+    p.len = (unsigned)((w.len - off) < chunk ? (w.len - off) : chunk);
+    items[first + k] = p;
+  }
+}
+
+// ------------------------------------------------------------------- exec
+__device__ __forceinline__ WorkItem load_item(const WorkItem *p) {
+  const uint4 *q = reinterpret_cast<const uint4 *>(p);
+  uint4 a = __ldg(q), b = __ldg(q + 1);
+  WorkItem w;
+  w.dst = ((unsigned long long)a.y << 32) | a.x;
+  w.src = ((unsigned long long)a.w << 32) | a.z;
+  w.len = b.x;
+  w.kind = b.y;
+  w.value = (int)b.z;
+  w.pad = b.w;
+  return w;
+}
+
+template <int VB, int U>
+__device__ __forceinline__ void run_item(const WorkItem &w, unsigned lane) {
+  if (w.kind == kCopy) {
+    copy_coop<VB, U>(reinterpret_cast<char *>(w.dst), reinterpret_cast<const char *>(w.src), w.len, lane, 32);
+  } else if (lane == 0) {
+    if (w.kind == kSignal) {
+      fence_gpu();
+      st_release_b32(reinterpret_cast<void *>(w.dst), (unsigned)w.value);
+    } else if (w.len == 8) {
+      st_relaxed_b64(reinterpret_cast<void *>(w.dst), w.src);
+    } else {
+      st_relaxed_b32(reinterpret_cast<void *>(w.dst), (unsigned)w.src);
+    }
+  }
+}
+
+template <int VB, int U>
+__global__ void __launch_bounds__(1024) batch_exec_kernel(const WorkItem *__restrict__ items, BatchCtl *ctl,
+                                                          unsigned long long cap, int grab) {
+  const unsigned lane = threadIdx.x & 31u;
+  if (*(volatile int *)&ctl->status != 0) return;
+  unsigned long long C = *(volatile unsigned long long *)&ctl->total_chunks;
+  if (C > cap) return;
+  unsigned long long base = 0;
+  if (lane == 0) base = atomicAdd(&ctl->cursor, (unsigned long long)grab);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  while (base < C) {
+    unsigned long long nxt = 0;
+    if (lane == 0) nxt = atomicAdd(&ctl->cursor, (unsigned long long)grab);
+    const unsigned long long end = base + grab < C ? base + grab : C;
+    WorkItem cur = load_item(items + base);
+    for (unsigned long long k = base; k < end; ++k) {
+      WorkItem nx;
+      if (k + 1 < end) nx = load_item(items + k + 1);
+      run_item<VB, U>(cur, lane);
+      cur = nx;
+    }
+    base = __shfl_sync(0xffffffffu, nxt, 0);
+  }
+}
+
+typedef void (*ExecFn)(const WorkItem *, BatchCtl *, unsigned long long, int);
+
+static ExecFn pick_exec(int vb, int u) {
+#define NVSHM_PICK(V, UU) \
+  if (vb == V && u == UU) return batch_exec_kernel<V, UU>;
+  NVSHM_PICK(16, 1) NVSHM_PICK(16, 2) NVSHM_PICK(16, 4) NVSHM_PICK(16, 8)
+  NVSHM_PICK(8, 1) NVSHM_PICK(8, 2) NVSHM_PICK(8, 4) NVSHM_PICK(8, 8)
+  NVSHM_PICK(4, 1) NVSHM_PICK(4, 2) NVSHM_PICK(4, 4) NVSHM_PICK(4, 8)
+#undef NVSHM_PICK
+  return nullptr;
+}
+
+int check_batch_config(const nvshmemx_batch_config &c) {
+  const bool ok = (c.vec_bytes == 4 || c.vec_bytes == 8 || c.vec_bytes == 16) && c.chunk_bytes >= 256 &&
+                  c.chunk_bytes <= (1 << 20) && (c.chunk_bytes % 256) == 0 &&
+                  (c.unroll == 1 || c.unroll == 2 || c.unroll == 4 || c.unroll == 8) &&
+                  (c.threads == 128 || c.threads == 256 || c.threads == 512 || c.threads == 1024) &&
+                  c.ctas_per_sm >= 0 && c.ctas_per_sm <= 16 && c.grab >= 1 && c.grab <= 16;
+  return ok ? 0 : NVSHMEMX_ERR_INVALID;
+}
+
+}  // namespace nvshm
+
+using namespace nvshm;
+
+struct nvshmemx_batch {
+  int max_n = 0;
+  int min_chunk = 256;
+  unsigned long long cap = 0;
+  nvshmemx_request *d_reqs = nullptr;
+  WorkItem *d_items = nullptr;
+  BatchCtl *d_ctl = nullptr;
+  nvshmemx_request *h_reqs = nullptr;  // pinned
+  int *h_status = nullptr;             // pinned
+  int n = 0;
+  nvshmemx_batch_config cfg{};
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int graph_n = -1;
+  nvshmemx_batch_config graph_cfg{};
+  Cfg graph_arena{};
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr, ev_plan0 = nullptr, ev_exec0 = nullptr, ev_exec1 = nullptr;
+  bool timed_graph = false;
+};
+
+static void drop_graph(nvshmemx_batch *b) {
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->gexec = nullptr;
+  b->graph = nullptr;
+  b->graph_n = -1;
+}
+
+// Enqueues memset + plan + exec on b->stream (used both for capture and for
+// the direct path).
+static int enqueue_batch(nvshmemx_batch *b, bool with_events) {
+  const Runtime &r = rt();
+  const Cfg c = r.cfg;
+  const nvshmemx_batch_config &k = b->cfg;
+  ExecFn fn = pick_exec(k.vec_bytes, k.unroll);
+  if (!fn) return fail(NVSHMEMX_ERR_INVALID, "batch: no kernel for vec %d unroll %d", k.vec_bytes, k.unroll);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, k.threads, 0);
+  if (per_sm < 1) per_sm = 1;
+  int ctas = k.ctas_per_sm > 0 && k.ctas_per_sm < per_sm ? k.ctas_per_sm : per_sm;
+  cudaMemsetAsync(b->d_ctl, 0, sizeof(BatchCtl), b->stream);
+  if (with_events) cudaEventRecord(b->ev_plan0, b->stream);
+  if (b->n > 0)
+    batch_plan_kernel<<<(b->n + 255) / 256, 256, 0, b->stream>>>(c, b->d_reqs, b->n, (unsigned)k.chunk_bytes,
+                                                                 b->d_items, b->cap, b->d_ctl);
+  if (with_events) cudaEventRecord(b->ev_exec0, b->stream);
+  fn<<<r.sm_count * ctas, k.threads, 0, b->stream>>>(b->d_items, b->d_ctl, b->cap, k.grab);
+  if (with_events) cudaEventRecord(b->ev_exec1, b->stream);
+  return check_cuda(cudaGetLastError(), "batch launch");
+}
+
+static int ensure_graph(nvshmemx_batch *b) {
+  const Cfg &c = rt().cfg;
+  if (b->gexec && b->graph_n == b->n && memcmp(&b->graph_cfg, &b->cfg, sizeof b->cfg) == 0 &&
+      memcmp(&b->graph_arena, &c, sizeof c) == 0)
+    return 0;
+  drop_graph(b);
+  int rc;
+  if ((rc = check_cuda(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture")))
+    return rc;
+  int erc = enqueue_batch(b, true);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  if (erc) {
+    if (g) cudaGraphDestroy(g);
+    return erc;
+  }
+  if ((rc = check_cuda(e, "cudaStreamEndCapture"))) return rc;
+  b->graph = g;
+  if ((rc = check_cuda(cudaGraphInstantiate(&b->gexec, g, 0), "cudaGraphInstantiate"))) {
+    drop_graph(b);
+    return rc;
+  }
+  b->graph_n = b->n;
+  b->graph_cfg = b->cfg;
+  b->graph_arena = c;
+  return 0;
+}
+
+extern "C" {
+
+void nvshmemx_batch_default_config(nvshmemx_batch_config *c) {
+  c->vec_bytes = 16;
+  c->chunk_bytes = 16384;
+  c->unroll = 4;
+  c->threads = 512;
+  c->ctas_per_sm = 2;
+  c->grab = 2;
+}
+
+int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes, int min_chunk_bytes,
+                          nvshmemx_batch **out) {
+  if (!is_started()) return fail(NVSHMEMX_ERR_STATE, "batch before nvstart_pes");
+  if (!out || max_requests < 1) return fail(NVSHMEMX_ERR_INVALID, "batch_create: bad arguments");
+  if (min_chunk_bytes < 256) min_chunk_bytes = 256;
+  nvshmemx_batch *b = new nvshmemx_batch();
+  b->max_n = max_requests;
+  b->min_chunk = min_chunk_bytes;
+  b->cap = (unsigned long long)max_requests + max_payload_bytes / (unsigned long long)min_chunk_bytes + 1;
+  nvshmemx_batch_default_config(&b->cfg);
+  if (b->cfg.chunk_bytes < min_chunk_bytes) b->cfg.chunk_bytes = (min_chunk_bytes + 255) / 256 * 256;
+  int rc = 0;
+  if ((rc = check_cuda(cudaMalloc(&b->d_reqs, (size_t)max_requests * sizeof(nvshmemx_request)), "cudaMalloc(reqs)")) ||
+      (rc = check_cuda(cudaMalloc(&b->d_items, (size_t)b->cap * sizeof(WorkItem)), "cudaMalloc(items)")) ||
+      (rc = check_cuda(cudaMalloc(&b->d_ctl, sizeof(BatchCtl)), "cudaMalloc(ctl)")) ||
+      (rc = check_cuda(cudaMallocHost(&b->h_reqs, (size_t)max_requests * sizeof(nvshmemx_request)),
+                       "cudaMallocHost(reqs)")) ||
+      (rc = check_cuda(cudaMallocHost(&b->h_status, 64), "cudaMallocHost(status)")) ||
+      (rc = check_cuda(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate"))) {
+    nvshmemx_batch_destroy(b);
+    return rc;
+  }
+  cudaEventCreate(&b->ev_start);
+  cudaEventCreate(&b->ev_stop);
+  cudaEventCreate(&b->ev_plan0);
+  cudaEventCreate(&b->ev_exec0);
+  cudaEventCreate(&b->ev_exec1);
+  cudaMemset(b->d_ctl, 0, sizeof(BatchCtl));
+  *out = b;
+  return 0;
+}
+
+int nvshmemx_batch_destroy(nvshmemx_batch *b) {
+  if (!b) return 0;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  drop_graph(b);
+  if (b->d_reqs) cudaFree(b->d_reqs);
+  if (b->d_items) cudaFree(b->d_items);
+  if (b->d_ctl) cudaFree(b->d_ctl);
+  if (b->h_reqs) cudaFreeHost(b->h_reqs);
+  if (b->h_status) cudaFreeHost(b->h_status);
+  cudaEvent_t evs[] = {b->ev_start, b->ev_stop, b->ev_plan0, b->ev_exec0, b->ev_exec1};
+  for (auto e : evs)
+    if (e) cudaEventDestroy(e);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return 0;
+}
+
+int nvshmemx_batch_set_config(nvshmemx_batch *b, const nvshmemx_batch_config *cfg) {
+  if (!b || !cfg || check_batch_config(*cfg) || cfg->chunk_bytes < b->min_chunk)
+    return fail(NVSHMEMX_ERR_INVALID, "batch_set_config: invalid configuration");
+  b->cfg = *cfg;
+  return 0;
+}
+
+int nvshmemx_batch_get_config(const nvshmemx_batch *b, nvshmemx_batch_config *cfg) {
+  if (!b || !cfg) return NVSHMEMX_ERR_INVALID;
+  *cfg = b->cfg;
+  return 0;
+}
+
+nvshmemx_request *nvshmemx_batch_host_buffer(nvshmemx_batch *b) { return b ? b->h_reqs : nullptr; }
+
+int nvshmemx_batch_upload(nvshmemx_batch *b, const nvshmemx_request *reqs, int n) {
+  if (!b || n < 0 || n > b->max_n) return fail(NVSHMEMX_ERR_INVALID, "batch_upload: n outside [0, max]");
+  int rc;
+  if (n &&
+      (rc = check_cuda(cudaMemcpyAsync(b->d_reqs, reqs, (size_t)n * sizeof(nvshmemx_request), cudaMemcpyHostToDevice,
+                                       b->stream),
+                       "cudaMemcpyAsync(requests)")))
+    return rc;
+  b->n = n;
+  return check_cuda(cudaStreamSynchronize(b->stream), "batch_upload");
+}
+
+int nvshmemx_batch_execute(nvshmemx_batch *b, int reps, float *out_ms) {
+  if (!b || reps < 1) return fail(NVSHMEMX_ERR_INVALID, "batch_execute: bad arguments");
+  int rc;
+  if ((rc = ensure_graph(b))) return rc;
+  cudaEventRecord(b->ev_start, b->stream);
+  for (int i = 0; i < reps; ++i)
+    if ((rc = check_cuda(cudaGraphLaunch(b->gexec, b->stream), "cudaGraphLaunch"))) return rc;
+  cudaEventRecord(b->ev_stop, b->stream);
+  if ((rc = check_cuda(cudaStreamSynchronize(b->stream), "batch_execute"))) return rc;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, b->ev_start, b->ev_stop);
+  if (out_ms) *out_ms = ms;
+  b->timed_graph = true;
+  int st[2] = {0, 0};
+  cudaMemcpy(st, &b->d_ctl->status, sizeof st, cudaMemcpyDeviceToHost);
+  if (st[0]) return fail(st[0], "batch_execute: request %d rejected (%s)", st[1], nvshmemx_strerror(st[0]));
+  return 0;
+}
+
+int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n, int *out_status, float *out_ms) {
+  if (!b || n < 0 || n > b->max_n) return fail(NVSHMEMX_ERR_INVALID, "batch_submit: n outside [0, max]");
+  int rc;
+  b->n = n;
+  if ((rc = ensure_graph(b))) return rc;
+  cudaEventRecord(b->ev_start, b->stream);
+  if (n &&
+      (rc = check_cuda(cudaMemcpyAsync(b->d_reqs, reqs, (size_t)n * sizeof(nvshmemx_request), cudaMemcpyHostToDevice,
+                                       b->stream),
+                       "cudaMemcpyAsync(requests)")))
+    return rc;
+  if ((rc = check_cuda(cudaGraphLaunch(b->gexec, b->stream), "cudaGraphLaunch"))) return rc;
+  if ((rc = check_cuda(cudaMemcpyAsync(b->h_status, &b->d_ctl->status, 8, cudaMemcpyDeviceToHost, b->stream),
+                       "cudaMemcpyAsync(status)")))
+    return rc;
+  cudaEventRecord(b->ev_stop, b->stream);
+  if ((rc = check_cuda(cudaStreamSynchronize(b->stream), "batch_submit"))) return rc;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, b->ev_start, b->ev_stop);
+  if (out_ms) *out_ms = ms;
+  if (out_status) *out_status = b->h_status[0];
+  b->timed_graph = true;
+  return 0;
+}
+
+int nvshmemx_batch_last_stats(const nvshmemx_batch *b, unsigned long long *chunks, float *plan_ms, float *exec_ms) {
+  if (!b) return NVSHMEMX_ERR_INVALID;
+  if (chunks) {
+    BatchCtl h;
+    cudaMemcpy(&h, b->d_ctl, sizeof h, cudaMemcpyDeviceToHost);
+    *chunks = h.total_chunks;
+  }
+  if (b->timed_graph) {
+    float p = 0, e = 0;
+    cudaEventElapsedTime(&p, b->ev_plan0, b->ev_exec0);
+    cudaEventElapsedTime(&e, b->ev_exec0, b->ev_exec1);
+    if (plan_ms) *plan_ms = p;
+    if (exec_ms) *exec_ms = e;
+  }
+  return 0;
+}
+
+unsigned long long nvshmemx_requests_bytes(const nvshmemx_request *reqs, int n) {
+  unsigned long long t = 0;
+  for (int i = 0; i < n; ++i) {
+    const nvshmemx_request &r = reqs[i];
+    const unsigned w = r.dtype == NVSHMEMX_DT_DOUBLE ? 8u : 4u;
+    switch (r.op) {
+      case NVSHMEMX_REQ_PUT:
+      case NVSHMEMX_REQ_GET: t += 2ull * r.bytes; break;
+      case NVSHMEMX_REQ_G: t += 2ull * w; break;
+      case NVSHMEMX_REQ_SIGNAL: t += 4; break;
+      case NVSHMEMX_REQ_P: t += w; break;
+      default: break;
+    }
+  }
+  return t;
+}
+
+// Per-call path on the batch's device-resident requests: one caller unit per
+// request through the public device API (nvshmemx_exec_requests' kernel).
+int nvshmemx_batch_execute_percall(nvshmemx_batch *b, int mode, int reps, float *out_ms) {
+  if (!b || reps < 1 || mode < 0 || mode > NVSHMEMX_MODE_BULK)
+    return fail(NVSHMEMX_ERR_INVALID, "batch_execute_percall: bad arguments");
+  int rc;
+  cudaEventRecord(b->ev_start, b->stream);
+  for (int i = 0; i < reps; ++i)
+    if ((rc = launch_exec_requests(mode, b->d_reqs, b->n, b->stream))) return rc;
+  cudaEventRecord(b->ev_stop, b->stream);
+  if ((rc = check_cuda(cudaStreamSynchronize(b->stream), "batch_execute_percall"))) return rc;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, b->ev_start, b->ev_stop);
+  if (out_ms) *out_ms = ms;
+  return 0;
+}
+
+}  // extern "C"

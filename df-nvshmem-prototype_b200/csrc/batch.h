@@ -1,0 +1,19 @@
+// batch.h -- internals shared by the batch engine, the autotuner and the
+// learned picker.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "nvshmemx_batch.h"
+#include "runtime.h"
+
+namespace nvshm {
+
+// Launches the one-caller-unit-per-request kernel of nvshmemx_exec_requests
+// on device-resident requests (ops.cu).
+int launch_exec_requests(int mode, const nvshmemx_request *d_reqs, int n, cudaStream_t stream);
+
+// Validates a batch configuration; returns 0 or NVSHMEMX_ERR_INVALID.
+int check_batch_config(const nvshmemx_batch_config &c);
+
+}  // namespace nvshm

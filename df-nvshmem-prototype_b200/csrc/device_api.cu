@@ -1,0 +1,279 @@
+// device_api.cu -- the extern "C" __device__ API of nvshmem_device.h and the
+// device extensions of nvshmemx.h, built with -rdc=true so application
+// kernels link against them exactly as against the prototype's libnvshmem.a
+// (Makefile:28-34 of the prototype).
+//
+// Each function reads the arena configuration from the __constant__ copy
+// nvshm_dcfg (written by nvstart_pes / nvshmemx_init_attr) and forwards to the
+// inline implementation in nvshm_core.cuh.
+#include "nvshm_core.cuh"
+#include "nvshmem_device.h"
+#include "nvshmemx.h"
+
+__constant__ nvshm::Cfg nvshm_dcfg;
+
+using nvshm::Cfg;
+
+#define CFG nvshm_dcfg
+
+namespace {
+
+template <typename T>
+__device__ __forceinline__ void put_thread(T *target, const T *source, int len, int pe, int op) {
+  const Cfg &c = CFG;
+  const unsigned long long bytes = nvshm::elem_bytes<T>(len);
+  if (!nvshm::check_remote(c, target, bytes, pe) || !nvshm::check_local(c, source, bytes)) return;
+  char *dst = nvshm::xlate(c, target, pe);
+  unsigned long long t0 = c.trace ? nvshm::gtimer() : 0;
+  nvshm::copy_coop<16, 4>(dst, reinterpret_cast<const char *>(source), bytes, 0, 1);
+  if (c.trace) nvshm::trace_rec(c, op, source, dst, bytes, pe, t0, nvshm::gtimer());
+}
+
+template <typename T>
+__device__ __forceinline__ void get_thread(T *target, const T *source, int len, int pe, int op) {
+  const Cfg &c = CFG;
+  const unsigned long long bytes = nvshm::elem_bytes<T>(len);
+  if (!nvshm::check_remote(c, source, bytes, pe) || !nvshm::check_local(c, target, bytes)) return;
+  const char *src = nvshm::xlate(c, source, pe);
+  unsigned long long t0 = c.trace ? nvshm::gtimer() : 0;
+  nvshm::copy_coop<16, 4>(reinterpret_cast<char *>(target), src, bytes, 0, 1);
+  if (c.trace) nvshm::trace_rec(c, op, target, src, bytes, pe, t0, nvshm::gtimer());
+}
+
+// Cooperative forms: `r` of `n` threads; bounds are checked by every thread
+// (same arguments, same answer) so all skip together.
+__device__ __forceinline__ void putmem_coop(void *target, const void *source, unsigned long long bytes,
+                                            int pe, unsigned r, unsigned n, int op) {
+  const Cfg &c = CFG;
+  if (!nvshm::check_remote(c, target, bytes, pe) || !nvshm::check_local(c, source, bytes)) return;
+  char *dst = nvshm::xlate(c, target, pe);
+  unsigned long long t0 = (c.trace && r == 0) ? nvshm::gtimer() : 0;
+  nvshm::copy_coop<16, 4>(dst, reinterpret_cast<const char *>(source), bytes, r, n);
+  if (c.trace && r == 0) nvshm::trace_rec(c, op, source, dst, bytes, pe, t0, nvshm::gtimer());
+}
+
+__device__ __forceinline__ void getmem_coop(void *target, const void *source, unsigned long long bytes,
+                                            int pe, unsigned r, unsigned n, int op) {
+  const Cfg &c = CFG;
+  if (!nvshm::check_remote(c, source, bytes, pe) || !nvshm::check_local(c, target, bytes)) return;
+  const char *src = nvshm::xlate(c, source, pe);
+  unsigned long long t0 = (c.trace && r == 0) ? nvshm::gtimer() : 0;
+  nvshm::copy_coop<16, 4>(reinterpret_cast<char *>(target), src, bytes, r, n);
+  if (c.trace && r == 0) nvshm::trace_rec(c, op, target, src, bytes, pe, t0, nvshm::gtimer());
+}
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+}  // namespace
+
+extern "C" {
+
+// ---------------------------------------------------------------- tracing scope
+// The ring needs no open/close: records are written as ops happen.  These
+// remain as the prototype's entry points (nvshmem_device.h:38-39) and mark
+// scope boundaries with a zero-byte record when tracing is on.
+__device__ void nvshmem_trace_begin(void) {
+  const Cfg &c = CFG;
+  if (c.trace) {
+    unsigned long long t = nvshm::gtimer();
+    nvshm::trace_rec(c, NVSHMEMX_TRACE_BEGIN, nullptr, nullptr, 0, nvshm::my_pe(), t, t);
+  }
+}
+__device__ void nvshmem_trace_end(void) {
+  const Cfg &c = CFG;
+  if (c.trace) {
+    unsigned long long t = nvshm::gtimer();
+    nvshm::trace_rec(c, NVSHMEMX_TRACE_END, nullptr, nullptr, 0, nvshm::my_pe(), t, t);
+  }
+}
+
+// nvshmem_device.cu:431-436: the prototype fenced at system scope for PCIe
+// peers; every PE here shares the GPU's L2, so a GPU-scope acq_rel fence
+// orders the caller's stores for every other PE.
+__device__ void nvshmem_quiet(void) { nvshm::fence_gpu(); }
+
+// nvshmem_device.cu:439-460
+__device__ void nvshmem_int_p(int *target, const int value, int pe) {
+  const Cfg &c = CFG;
+  nvshm::p_one<int>(c, target, value, pe);
+  if (c.trace) {
+    unsigned long long t = nvshm::gtimer();
+    nvshm::trace_rec(c, NVSHMEMX_TRACE_PUT_INT, nullptr, target, 4, pe, t, t);
+  }
+}
+__device__ void nvshmem_float_p(float *target, const float value, int pe) {
+  const Cfg &c = CFG;
+  nvshm::p_one<float>(c, target, value, pe);
+  if (c.trace) {
+    unsigned long long t = nvshm::gtimer();
+    nvshm::trace_rec(c, NVSHMEMX_TRACE_PUT_FLOAT, nullptr, target, 4, pe, t, t);
+  }
+}
+__device__ void nvshmem_double_p(double *target, const double value, int pe) {
+  const Cfg &c = CFG;
+  nvshm::p_one<double>(c, target, value, pe);
+  if (c.trace) {
+    unsigned long long t = nvshm::gtimer();
+    nvshm::trace_rec(c, NVSHMEMX_TRACE_PUT_DOUBLE, nullptr, target, 8, pe, t, t);
+  }
+}
+
+// nvshmem_device.cu:463-485
+__device__ int nvshmem_int_g(int *source, int pe) {
+  const Cfg &c = CFG;
+  int v = nvshm::g_one<int>(c, source, pe);
+  if (c.trace) {
+    unsigned long long t = nvshm::gtimer();
+    nvshm::trace_rec(c, NVSHMEMX_TRACE_GET_INT, nullptr, source, 4, pe, t, t);
+  }
+  return v;
+}
+__device__ float nvshmem_float_g(float *source, int pe) {
+  const Cfg &c = CFG;
+  float v = nvshm::g_one<float>(c, source, pe);
+  if (c.trace) {
+    unsigned long long t = nvshm::gtimer();
+    nvshm::trace_rec(c, NVSHMEMX_TRACE_GET_FLOAT, nullptr, source, 4, pe, t, t);
+  }
+  return v;
+}
+__device__ double nvshmem_double_g(double *source, int pe) {
+  const Cfg &c = CFG;
+  double v = nvshm::g_one<double>(c, source, pe);
+  if (c.trace) {
+    unsigned long long t = nvshm::gtimer();
+    nvshm::trace_rec(c, NVSHMEMX_TRACE_GET_DOUBLE, nullptr, source, 8, pe, t, t);
+  }
+  return v;
+}
+
+// nvshmem_device.cu:488-512 (one thread copies all `len` elements, 16-byte
+// vectors for the aligned body instead of one volatile element per store)
+__device__ void nvshmem_int_put(int *target, int *source, int len, int pe) {
+  put_thread<int>(target, source, len, pe, NVSHMEMX_TRACE_PUT_INT);
+}
+__device__ void nvshmem_float_put(float *target, float *source, int len, int pe) {
+  put_thread<float>(target, source, len, pe, NVSHMEMX_TRACE_PUT_FLOAT);
+}
+__device__ void nvshmem_double_put(double *target, double *source, int len, int pe) {
+  put_thread<double>(target, source, len, pe, NVSHMEMX_TRACE_PUT_DOUBLE);
+}
+
+// nvshmem_device.cu:515-540
+__device__ void nvshmem_int_get(int *target, int *source, int len, int pe) {
+  get_thread<int>(target, source, len, pe, NVSHMEMX_TRACE_GET_INT);
+}
+__device__ void nvshmem_float_get(float *target, float *source, int len, int pe) {
+  get_thread<float>(target, source, len, pe, NVSHMEMX_TRACE_GET_FLOAT);
+}
+__device__ void nvshmem_double_get(double *target, double *source, int len, int pe) {
+  get_thread<double>(target, source, len, pe, NVSHMEMX_TRACE_GET_DOUBLE);
+}
+
+// nvshmem_device.cu:542-562: returns once *ivar != cmp_value.
+__device__ void nvshmem_int_wait(int *ivar, int cmp_value) {
+  const Cfg &c = CFG;
+  unsigned long long t0 = c.trace ? nvshm::gtimer() : 0;
+  nvshm::wait_cmp(c, ivar, NVSHMEMX_CMP_NE, cmp_value, 0);
+  if (c.trace) nvshm::trace_rec(c, NVSHMEMX_TRACE_WAIT_INT, ivar, nullptr, 4, nvshm::my_pe(), t0, nvshm::gtimer());
+}
+
+// nvshmem_device.cu:564-584: returns once *ivar == cmp_value; `cmp` is
+// ignored exactly as in the prototype.
+__device__ void nvshmem_int_wait_until(int *ivar, int cmp, int cmp_value) {
+  (void)cmp;
+  const Cfg &c = CFG;
+  unsigned long long t0 = c.trace ? nvshm::gtimer() : 0;
+  nvshm::wait_cmp(c, ivar, NVSHMEMX_CMP_EQ, cmp_value, 0);
+  if (c.trace)
+    nvshm::trace_rec(c, NVSHMEMX_TRACE_WAIT_UNTIL_INT, ivar, nullptr, 4, nvshm::my_pe(), t0, nvshm::gtimer());
+}
+
+// ---------------------------------------------------------------- extensions
+__device__ int nvshmemx_my_pe(void) { return nvshm::my_pe(); }
+__device__ int nvshmemx_n_pes(void) { return CFG.npes; }
+
+__device__ void *nvshmemx_ptr(const void *sym, int pe) {
+  const Cfg &c = CFG;
+  if (!nvshm::in_arena(c, sym) || (unsigned)pe >= (unsigned)c.npes) return nullptr;
+  return nvshm::xlate(c, sym, pe);
+}
+__device__ void *nvshmemx_local_ptr(const void *sym) { return nvshmemx_ptr(sym, nvshm::my_pe()); }
+
+__device__ void nvshmemx_putmem_warp(void *target, const void *source, size_t bytes, int pe) {
+  putmem_coop(target, source, bytes, pe, lane_id(), 32, NVSHMEMX_TRACE_PUT_INT);
+}
+__device__ void nvshmemx_getmem_warp(void *target, const void *source, size_t bytes, int pe) {
+  getmem_coop(target, source, bytes, pe, lane_id(), 32, NVSHMEMX_TRACE_GET_INT);
+}
+__device__ void nvshmemx_putmem_block(void *target, const void *source, size_t bytes, int pe) {
+  putmem_coop(target, source, bytes, pe, nvshm::block_rank(), nvshm::block_size(), NVSHMEMX_TRACE_PUT_INT);
+}
+__device__ void nvshmemx_getmem_block(void *target, const void *source, size_t bytes, int pe) {
+  getmem_coop(target, source, bytes, pe, nvshm::block_rank(), nvshm::block_size(), NVSHMEMX_TRACE_GET_INT);
+}
+
+#define NVSHM_TYPED_COOP(Name, Type, OPP, OPG)                                                 \
+  __device__ void nvshmemx_##Name##_put_warp(Type *t, Type *s, int len, int pe) {             \
+    putmem_coop(t, s, nvshm::elem_bytes<Type>(len), pe, lane_id(), 32, OPP);                  \
+  }                                                                                           \
+  __device__ void nvshmemx_##Name##_get_warp(Type *t, Type *s, int len, int pe) {             \
+    getmem_coop(t, s, nvshm::elem_bytes<Type>(len), pe, lane_id(), 32, OPG);                  \
+  }                                                                                           \
+  __device__ void nvshmemx_##Name##_put_block(Type *t, Type *s, int len, int pe) {            \
+    putmem_coop(t, s, nvshm::elem_bytes<Type>(len), pe, nvshm::block_rank(), nvshm::block_size(), \
+                OPP);                                                                         \
+  }                                                                                           \
+  __device__ void nvshmemx_##Name##_get_block(Type *t, Type *s, int len, int pe) {            \
+    getmem_coop(t, s, nvshm::elem_bytes<Type>(len), pe, nvshm::block_rank(), nvshm::block_size(), \
+                OPG);                                                                         \
+  }
+
+NVSHM_TYPED_COOP(int, int, NVSHMEMX_TRACE_PUT_INT, NVSHMEMX_TRACE_GET_INT)
+NVSHM_TYPED_COOP(float, float, NVSHMEMX_TRACE_PUT_FLOAT, NVSHMEMX_TRACE_GET_FLOAT)
+NVSHM_TYPED_COOP(double, double, NVSHMEMX_TRACE_PUT_DOUBLE, NVSHMEMX_TRACE_GET_DOUBLE)
+#undef NVSHM_TYPED_COOP
+
+__device__ void nvshmemx_putmem_bulk_block(void *target, const void *source, size_t bytes, int pe,
+                                           void *smem, unsigned int smem_bytes) {
+  const Cfg &c = CFG;
+  if (!nvshm::check_remote(c, target, bytes, pe) || !nvshm::check_local(c, source, bytes)) return;
+  nvshm::bulk_copy_block(c, nvshm::xlate(c, target, pe), reinterpret_cast<const char *>(source), bytes,
+                         smem, smem_bytes);
+}
+__device__ void nvshmemx_getmem_bulk_block(void *target, const void *source, size_t bytes, int pe,
+                                           void *smem, unsigned int smem_bytes) {
+  const Cfg &c = CFG;
+  if (!nvshm::check_remote(c, source, bytes, pe) || !nvshm::check_local(c, target, bytes)) return;
+  nvshm::bulk_copy_block(c, reinterpret_cast<char *>(target), nvshm::xlate(c, source, pe), bytes, smem,
+                         smem_bytes);
+}
+
+__device__ void nvshmemx_int_signal(int *target, int value, int pe) {
+  const Cfg &c = CFG;
+  if (!nvshm::check_remote(c, target, 4, pe) || !nvshm::check_align(c, target, 4)) return;
+  nvshm::st_release_b32(nvshm::xlate(c, target, pe), (unsigned)value);
+}
+
+__device__ int nvshmemx_int_wait_until_cmp(int *ivar, int cmp, int value, long long timeout_ns) {
+  return nvshm::wait_cmp(CFG, ivar, cmp, value, timeout_ns);
+}
+
+__device__ int nvshmemx_barrier_all(void) {
+  const Cfg &c = CFG;
+  unsigned long long t0 = c.trace ? nvshm::gtimer() : 0;
+  int rc = nvshm::barrier_all(c);
+  if (c.trace && nvshm::block_rank() == 0)
+    nvshm::trace_rec(c, NVSHMEMX_TRACE_BARRIER, nullptr, nullptr, 0, nvshm::my_pe(), t0, nvshm::gtimer());
+  return rc;
+}
+__device__ int nvshmemx_barrier_pe(void) { return nvshm::barrier_pe(CFG); }
+
+}  // extern "C"
+
+namespace nvshm {
+// Host side: publish the arena configuration to the __constant__ copy read by
+// the public device API (replaces initialize_cuda_constants,
+// nvshmem_cuda_constants.cu:52-57).
+cudaError_t upload_cfg(const Cfg &c) { return cudaMemcpyToSymbol(nvshm_dcfg, &c, sizeof(Cfg)); }
+}  // namespace nvshm

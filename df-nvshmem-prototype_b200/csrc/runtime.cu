@@ -1,0 +1,770 @@
+// runtime.cu -- host runtime of the virtual-PE library: arena set-up,
+// symmetric allocation, address queries, host and offload barriers, the
+// collective launcher, SPMD host threads, status and the trace ring.
+//
+// The prototype's equivalents live in nvshmem.cu (nvstart_pes :472-773,
+// nvshmalloc :775-802, nvshmcleanup :805-819, nvstop_pes :821-856,
+// nvshmem_barrier_all :858-867, nvshmem_barrier_all_offload :869-878,
+// nvshmem_ptr :880-883) and nvshmem_kernels.cu:56-102.  There, every PE is a
+// process that maps its peers' heaps over CUDA IPC after an MPI exchange.
+// Here every PE is a slice of one arena on one GPU, so the exchange and the
+// IPC mappings disappear: set-up is one reservation of address space, one
+// physical allocation per slice and one upload of the configuration.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+
+#include <chrono>
+#include <condition_variable>
+#include <string>
+#include <thread>
+
+#include "nvshmem.h"
+#include "nvshmemx.h"
+#include "runtime.h"
+
+namespace nvshm {
+
+thread_local int t_pe = 0;
+thread_local bool t_spmd = false;
+
+Runtime &rt() {
+  static Runtime r;
+  return r;
+}
+const Cfg &cfg() { return rt().cfg; }
+bool is_started() { return rt().started; }
+
+static bool env_error_mode_read = false;
+
+static void read_env_error_mode() {
+  if (env_error_mode_read) return;
+  env_error_mode_read = true;
+  const char *m = getenv("NVSHMEM_ERROR_MODE");
+  if (m && strcmp(m, "return") == 0) rt().error_mode = NVSHMEMX_ERRORS_RETURN;
+}
+
+int fail(int code, const char *fmt, ...) {
+  Runtime &r = rt();
+  read_env_error_mode();
+  char msg[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(msg, sizeof msg, fmt, ap);
+  va_end(ap);
+  if (r.host_err == 0) r.host_err = code;
+  if (r.error_mode == NVSHMEMX_ERRORS_EXIT) {
+    fprintf(stderr, "[nvshmem %d] %s\n", t_pe, msg);
+    exit(-1);
+  }
+  if (getenv("NVSHMEM_DEBUG")) fprintf(stderr, "[nvshmem %d] %s\n", t_pe, msg);
+  return code;
+}
+
+int check_cuda(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return NVSHMEMX_SUCCESS;
+  return fail(NVSHMEMX_ERR_CUDA, "%s failed: %s", what, cudaGetErrorString(e));
+}
+
+// Driver entry points for the virtual-memory calls, resolved through the
+// runtime (cudaGetDriverEntryPoint) so the shared library carries no link-time
+// dependency on libcuda and loads on machines without a GPU driver.
+struct DriverApi {
+  PFN_cuGetErrorString get_error_string = nullptr;
+  PFN_cuMemGetAllocationGranularity granularity = nullptr;
+  PFN_cuMemAddressReserve reserve = nullptr;
+  PFN_cuMemAddressFree address_free = nullptr;
+  PFN_cuMemCreate create = nullptr;
+  PFN_cuMemRelease release = nullptr;
+  PFN_cuMemMap map = nullptr;
+  PFN_cuMemUnmap unmap = nullptr;
+  PFN_cuMemSetAccess set_access = nullptr;
+  bool loaded = false;
+};
+static DriverApi g_drv;
+
+static bool get_entry(const char *name, void **fn) {
+  cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+  return cudaGetDriverEntryPoint(name, fn, cudaEnableDefault, &q) == cudaSuccess &&
+         q == cudaDriverEntryPointSuccess && *fn != nullptr;
+}
+
+static int load_driver() {
+  if (g_drv.loaded) return 0;
+  bool ok = get_entry("cuGetErrorString", (void **)&g_drv.get_error_string) &&
+            get_entry("cuMemGetAllocationGranularity", (void **)&g_drv.granularity) &&
+            get_entry("cuMemAddressReserve", (void **)&g_drv.reserve) &&
+            get_entry("cuMemAddressFree", (void **)&g_drv.address_free) &&
+            get_entry("cuMemCreate", (void **)&g_drv.create) &&
+            get_entry("cuMemRelease", (void **)&g_drv.release) &&
+            get_entry("cuMemMap", (void **)&g_drv.map) &&
+            get_entry("cuMemUnmap", (void **)&g_drv.unmap) &&
+            get_entry("cuMemSetAccess", (void **)&g_drv.set_access);
+  if (!ok) return fail(NVSHMEMX_ERR_CUDA, "cannot resolve the CUDA driver's virtual-memory entry points");
+  g_drv.loaded = true;
+  return 0;
+}
+
+static int check_cu(CUresult e, const char *what) {
+  if (e == CUDA_SUCCESS) return NVSHMEMX_SUCCESS;
+  const char *s = nullptr;
+  if (g_drv.get_error_string) g_drv.get_error_string(e, &s);
+  return fail(NVSHMEMX_ERR_CUDA, "%s failed: %s", what, s ? s : "?");
+}
+
+int publish_cfg() { return check_cuda(upload_cfg(rt().cfg), "cudaMemcpyToSymbol(cfg)"); }
+
+// ------------------------------------------------------------ offload barrier
+// One CTA per PE meets on a ticket counter that lives as long as the runtime
+// (P = npes never changes, so it needs no reset).  Replaces the prototype's
+// gather/release through PE 0 (nvshmem_kernels.cu:56-93), whose timeout
+// printed and carried on unsynchronised; here a timeout is recorded in the
+// status word.
+__global__ void offload_barrier_kernel(Cfg c, unsigned long long *ctr) {
+  unsigned long long t0 = c.trace ? gtimer() : 0;
+  ticket_barrier(c, ctr, (unsigned long long)gridDim.x);
+  if (c.trace && threadIdx.x == 0) {
+    int pe = (int)blockIdx.x;
+    unsigned long long idx = atomicAdd(&c.trace_head[pe], 1ull);
+    nvshmemx_trace_record *rec = c.trace + (size_t)pe * c.trace_cap + (size_t)(idx & (c.trace_cap - 1));
+    rec->t_ns = (long long)t0;
+    rec->spin_ns = (long long)(gtimer() - t0);
+    rec->local_addr = 0;
+    rec->remote_addr = 0;
+    rec->bytes = 0;
+    rec->op = NVSHMEMX_TRACE_BARRIER;
+    rec->pe = (unsigned short)pe;
+    rec->peer = (unsigned short)pe;
+    rec->tid = 0;
+    rec->block = 0;
+  }
+}
+
+// -------------------------------------------------------------- host barrier
+// Meeting point of the SPMD PE threads (stands in for MPI_Barrier).  A PE
+// thread that has returned, or a wait longer than the host deadline, fails the
+// barrier instead of hanging the others.
+struct HostBarrier {
+  std::mutex m;
+  std::condition_variable cv;
+  int n = 0, count = 0, departed = 0;
+  unsigned long long gen = 0;
+  int wait(double timeout_s) {
+    std::unique_lock<std::mutex> lk(m);
+    if (departed > 0) return NVSHMEMX_ERR_STATE;
+    unsigned long long g = gen;
+    if (++count == n) {
+      count = 0;
+      ++gen;
+      cv.notify_all();
+      return 0;
+    }
+    bool ok = cv.wait_for(lk, std::chrono::duration<double>(timeout_s),
+                          [&] { return gen != g || departed > 0; });
+    if (gen != g) return 0;
+    --count;
+    return ok ? NVSHMEMX_ERR_STATE : NVSHMEMX_ERR_TIMEOUT;
+  }
+  void depart() {
+    std::lock_guard<std::mutex> lk(m);
+    ++departed;
+    cv.notify_all();
+  }
+};
+static HostBarrier g_hbar;
+static std::vector<cudaEvent_t> g_spmd_events;
+
+static double host_barrier_timeout_s() {
+  const char *v = getenv("NVSHMEM_HOST_BARRIER_TIMEOUT_S");
+  return v ? atof(v) : 120.0;
+}
+
+// ---------------------------------------------------------------- set-up
+static size_t next_pow2(size_t x) {
+  size_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+static void release_all() {
+  Runtime &r = rt();
+  if (r.d_trace) cudaFree(r.d_trace);
+  if (r.d_trace_head) cudaFree(r.d_trace_head);
+  r.d_trace = nullptr;
+  r.d_trace_head = nullptr;
+  r.trace_cap = 0;
+  if (r.ctrl) cudaFree(r.ctrl);
+  r.ctrl = nullptr;
+  if (r.arena) {
+    for (int p = 0; p < (int)r.handles.size(); ++p) {
+      g_drv.unmap((CUdeviceptr)(r.arena + (size_t)p * r.stride), r.slice_mapped);
+      g_drv.release(r.handles[p]);
+    }
+    g_drv.address_free((CUdeviceptr)r.arena, (size_t)r.npes * r.stride);
+  }
+  r.handles.clear();
+  r.arena = nullptr;
+  r.started = false;
+}
+
+static int init_impl(int npes, size_t heap) {
+  Runtime &r = rt();
+  std::lock_guard<std::recursive_mutex> lk(r.mu);
+  read_env_error_mode();
+  if (r.started) return fail(NVSHMEMX_ERR_STATE, "nvstart_pes: already started");
+  if (npes < 1 || npes > NVSHMEMX_MAX_NPES)
+    return fail(NVSHMEMX_ERR_INVALID, "nvstart_pes: npes %d outside [1, %d]", npes, NVSHMEMX_MAX_NPES);
+  if (heap == 0) return fail(NVSHMEMX_ERR_INVALID, "nvstart_pes: heap size 0");
+  const char *to = getenv("NVSHMEM_WAIT_TIMEOUT_NS");
+  if (to) r.wait_timeout_ns = atoll(to);
+
+  int rc;
+  if ((rc = check_cuda(cudaFree(0), "cudaFree(0)"))) return rc;  // create the context
+  if ((rc = check_cuda(cudaGetDevice(&r.device), "cudaGetDevice"))) return rc;
+  if ((rc = load_driver())) return rc;
+  if ((rc = check_cuda(cudaDeviceGetAttribute(&r.sm_count, cudaDevAttrMultiProcessorCount, r.device),
+                       "cudaDeviceGetAttribute")))
+    return rc;
+
+  CUmemAllocationProp prop;
+  memset(&prop, 0, sizeof prop);
+  prop.type = CU_MEM_ALLOCATION_TYPE_PINNED;
+  prop.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
+  prop.location.id = r.device;
+  size_t gran = 0;
+  if ((rc = check_cu(g_drv.granularity(&gran, &prop, CU_MEM_ALLOC_GRANULARITY_RECOMMENDED),
+                     "cuMemGetAllocationGranularity")))
+    return rc;
+  r.npes = npes;
+  r.heap_bytes = heap;
+  r.slice_mapped = (heap + gran - 1) / gran * gran;
+  r.stride = next_pow2(r.slice_mapped);
+  r.log2_stride = 0;
+  while ((size_t(1) << r.log2_stride) < r.stride) ++r.log2_stride;
+
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  if ((size_t)npes * r.slice_mapped > free_b)
+    return fail(NVSHMEMX_ERR_NOMEM, "nvstart_pes: %d PEs x %zu bytes exceed free device memory (%zu)", npes,
+                r.slice_mapped, free_b);
+
+  CUdeviceptr base = 0;
+  if ((rc = check_cu(g_drv.reserve(&base, (size_t)npes * r.stride, r.stride, 0, 0),
+                     "cuMemAddressReserve")))
+    return rc;
+  r.arena = (char *)base;
+  r.handles.assign(npes, 0);
+  CUmemAccessDesc acc;
+  memset(&acc, 0, sizeof acc);
+  acc.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
+  acc.location.id = r.device;
+  acc.flags = CU_MEM_ACCESS_FLAGS_PROT_READWRITE;
+  for (int p = 0; p < npes; ++p) {
+    CUdeviceptr at = base + (size_t)p * r.stride;
+    if ((rc = check_cu(g_drv.create(&r.handles[p], r.slice_mapped, &prop, 0), "cuMemCreate")) ||
+        (rc = check_cu(g_drv.map(at, r.slice_mapped, 0, r.handles[p], 0), "cuMemMap")) ||
+        (rc = check_cu(g_drv.set_access(at, r.slice_mapped, &acc, 1), "cuMemSetAccess"))) {
+      r.handles.resize(p + 1);
+      if (r.handles[p] == 0) r.handles.resize(p);
+      release_all();
+      return rc;
+    }
+  }
+  // The prototype leaves its heap uninitialised (cuMemAlloc, nvshmem.cu:504);
+  // zeroing it makes every run start from the same heap image.
+  for (int p = 0; p < npes; ++p) {
+    if ((rc = check_cuda(cudaMemset(r.arena + (size_t)p * r.stride, 0, r.slice_mapped), "cudaMemset(arena)"))) {
+      release_all();
+      return rc;
+    }
+  }
+
+  // control block: status (64 B), collective counter and per-PE counters each
+  // on its own 128-byte line, then the offload-barrier counter.
+  const size_t line = 128;
+  size_t ctrl_bytes = line + line + (size_t)npes * line + line;
+  if ((rc = check_cuda(cudaMalloc(&r.ctrl, ctrl_bytes), "cudaMalloc(ctrl)"))) {
+    release_all();
+    return rc;
+  }
+  cudaMemset(r.ctrl, 0, ctrl_bytes);
+  r.d_status = (int *)r.ctrl;
+  r.d_coll_bar = (unsigned long long *)(r.ctrl + line);
+  r.d_pe_bar = (unsigned long long *)(r.ctrl + 2 * line);
+  r.d_offload_bar = (unsigned long long *)(r.ctrl + 2 * line + (size_t)npes * line);
+  r.bar_reset_bytes = line + (size_t)npes * line;
+  r.tail.assign(npes, 0);
+
+  Cfg &c = r.cfg;
+  memset(&c, 0, sizeof c);
+  c.arena = r.arena;
+  c.arena_bytes = (unsigned long long)npes * r.stride;
+  c.mask = r.stride - 1;
+  c.slice_bytes = r.heap_bytes;  // accesses stay inside NVSHMEM_HEAP_SIZE
+  c.log2_stride = r.log2_stride;
+  c.npes = npes;
+  c.status = r.d_status;
+  c.coll_bar = r.d_coll_bar;
+  // per-PE counters are 128 bytes apart: index p*16 in units of u64
+  c.pe_bar = r.d_pe_bar;
+  c.wait_timeout_ns = r.wait_timeout_ns;
+  r.started = true;
+  if ((rc = publish_cfg())) {
+    release_all();
+    return rc;
+  }
+  if ((rc = check_cuda(cudaDeviceSynchronize(), "cudaDeviceSynchronize"))) {
+    release_all();
+    return rc;
+  }
+  return NVSHMEMX_SUCCESS;
+}
+
+int launch_collective(const void *func, dim3 grid, dim3 block, void **args, size_t smem, cudaStream_t stream) {
+  Runtime &r = rt();
+  if (!r.started) return fail(NVSHMEMX_ERR_STATE, "collective launch before nvstart_pes");
+  if (grid.z != 1 || grid.x == 0 || grid.y == 0)
+    return fail(NVSHMEMX_ERR_INVALID, "collective launch: grid.z must be 1 (it carries the PE)");
+  int threads = (int)(block.x * block.y * block.z);
+  int rc;
+  if (smem > 48 * 1024) {
+    if ((rc = check_cuda(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                         "cudaFuncSetAttribute")))
+      return rc;
+  }
+  int per_sm = 0;
+  if ((rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, threads, smem),
+                       "cudaOccupancyMaxActiveBlocksPerMultiprocessor")))
+    return rc;
+  long long total = (long long)grid.x * grid.y * r.npes;
+  if (total > (long long)per_sm * r.sm_count)
+    return fail(NVSHMEMX_ERR_COOP, "collective launch: %lld CTAs cannot be co-resident (%d per SM x %d SMs)",
+                total, per_sm, r.sm_count);
+  if ((rc = check_cuda(cudaMemsetAsync(r.d_coll_bar, 0, r.bar_reset_bytes, stream), "cudaMemsetAsync(barrier)")))
+    return rc;
+  dim3 g(grid.x, grid.y, (unsigned)r.npes);
+  return check_cuda(cudaLaunchCooperativeKernel(func, g, block, args, smem, stream), "cudaLaunchCooperativeKernel");
+}
+
+int max_ctas_per_pe(const void *func, int block_threads, size_t smem) {
+  Runtime &r = rt();
+  if (!r.started) return 0;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, block_threads, smem) != cudaSuccess) return 0;
+  return per_sm * r.sm_count / r.npes;
+}
+
+}  // namespace nvshm
+
+using namespace nvshm;
+
+extern "C" {
+
+// ------------------------------------------------------------------ lifetime
+int nvshmemx_init_attr(int npes, size_t heap_bytes_per_pe) { return init_impl(npes, heap_bytes_per_pe); }
+
+void nvstart_pes(void) {
+  read_env_error_mode();
+  int npes = 2;
+  size_t heap = (size_t)1 << 30;  // HEAP_SIZE, nvshmem.cu:107
+  const char *v = getenv("NVSHMEM_NPES");
+  if (v) npes = atoi(v);
+  // The prototype read NVSHMEM_HEAP_SIZE only after allocating its heap
+  // (nvshmem.cu:504 vs :532), so the variable moved the bounds check but not
+  // the allocation; here it sizes the allocation too.
+  v = getenv("NVSHMEM_HEAP_SIZE");
+  if (v) heap = (size_t)atoll(v);
+  init_impl(npes, heap);
+}
+
+int nvshmemx_finalize(void) {
+  Runtime &r = rt();
+  std::lock_guard<std::recursive_mutex> lk(r.mu);
+  if (!r.started) return fail(NVSHMEMX_ERR_STATE, "nvstop_pes: not started");
+  int rc = check_cuda(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+  release_all();
+  return rc;
+}
+
+void nvstop_pes(void) {
+  if (t_spmd) {
+    // every PE thread calls it; the launching thread releases after the join
+    nvshmem_barrier_all();
+    return;
+  }
+  nvshmemx_finalize();
+}
+
+int nvshmemx_is_started(void) { return rt().started ? 1 : 0; }
+
+int nvshmem_my_pe(void) { return t_pe; }
+int nvshmem_n_pes(void) { return rt().npes; }
+
+// ---------------------------------------------------------------- allocation
+void *nvshmalloc(size_t size) {
+  Runtime &r = rt();
+  std::lock_guard<std::recursive_mutex> lk(r.mu);
+  if (!r.started) {
+    fail(NVSHMEMX_ERR_STATE, "nvshmalloc before nvstart_pes");
+    return nullptr;
+  }
+  if (t_spmd) {
+    size_t off = r.tail[t_pe];
+    if (off + size > r.heap_bytes) {
+      fail(NVSHMEMX_ERR_NOMEM,
+           "Not enough memory on the heap (set to %zu, can be increased by setting NVSHMEM_HEAP_SIZE)",
+           r.heap_bytes);
+      return nullptr;
+    }
+    r.tail[t_pe] = off + size;
+    return r.arena + (size_t)t_pe * r.stride + off;
+  }
+  // Called outside SPMD threads the allocation is collective by construction:
+  // every slice gets the same offset.
+  size_t off = r.tail[0];
+  for (int p = 1; p < r.npes; ++p) {
+    if (r.tail[p] != off) {
+      fail(NVSHMEMX_ERR_INVALID, "nvshmalloc: heap tails differ between PEs (asymmetric allocations)");
+      return nullptr;
+    }
+  }
+  if (off + size > r.heap_bytes) {
+    fail(NVSHMEMX_ERR_NOMEM,
+         "Not enough memory on the heap (set to %zu, can be increased by setting NVSHMEM_HEAP_SIZE)",
+         r.heap_bytes);
+    return nullptr;
+  }
+  for (int p = 0; p < r.npes; ++p) r.tail[p] = off + size;
+  return r.arena + (size_t)t_pe * r.stride + off;
+}
+
+void nvshmcleanup(void) {
+  Runtime &r = rt();
+  std::lock_guard<std::recursive_mutex> lk(r.mu);
+  if (!r.started) return;
+  if (t_spmd)
+    r.tail[t_pe] = 0;
+  else
+    for (auto &t : r.tail) t = 0;
+}
+
+void *nvshmem_ptr(void *local, int pe) {
+  Runtime &r = rt();
+  if (!r.started) return nullptr;
+  unsigned long long d = (unsigned long long)((char *)local - r.arena);
+  if (d >= (unsigned long long)r.npes * r.stride || pe < 0 || pe >= r.npes) return nullptr;
+  return r.arena + (size_t)pe * r.stride + (d & (r.stride - 1));
+}
+
+// ------------------------------------------------------------------ barriers
+void nvshmem_barrier_all(void) {
+  Runtime &r = rt();
+  if (!r.started) {
+    fail(NVSHMEMX_ERR_STATE, "nvshmem_barrier_all before nvstart_pes");
+    return;
+  }
+  if (check_cuda(cudaDeviceSynchronize(), "cudaDeviceSynchronize")) return;
+  if (t_spmd) {
+    int rc = g_hbar.wait(host_barrier_timeout_s());
+    if (rc) fail(rc, "nvshmem_barrier_all: a PE thread left or the host barrier timed out");
+  }
+}
+
+void nvshmem_barrier_all_offload(void) {
+  Runtime &r = rt();
+  if (!r.started) {
+    fail(NVSHMEMX_ERR_STATE, "nvshmem_barrier_all_offload before nvstart_pes");
+    return;
+  }
+  if (t_spmd) {
+    // Each PE thread's stream waits for every PE's earlier work: record, meet
+    // on the host (no GPU wait), then wait on all events, then meet again so
+    // no event is re-recorded before everyone has enqueued its waits.
+    if (check_cuda(cudaEventRecord(g_spmd_events[t_pe], 0), "cudaEventRecord")) return;
+    int rc = g_hbar.wait(host_barrier_timeout_s());
+    if (rc) {
+      fail(rc, "nvshmem_barrier_all_offload: a PE thread left or the host barrier timed out");
+      return;
+    }
+    for (int p = 0; p < r.npes; ++p)
+      if (check_cuda(cudaStreamWaitEvent(0, g_spmd_events[p], 0), "cudaStreamWaitEvent")) return;
+    rc = g_hbar.wait(host_barrier_timeout_s());
+    if (rc) fail(rc, "nvshmem_barrier_all_offload: a PE thread left or the host barrier timed out");
+    return;
+  }
+  Cfg c = r.cfg;
+  unsigned long long *ctr = r.d_offload_bar;
+  void *args[] = {&c, &ctr};
+  check_cuda(cudaLaunchCooperativeKernel((const void *)offload_barrier_kernel, dim3(r.npes), dim3(32), args, 0, 0),
+             "cudaLaunchCooperativeKernel(offload barrier)");
+}
+
+// ---------------------------------------------------------- collective launch
+int nvshmemx_collective_launch(const void *func, dim3 grid_per_pe, dim3 block, void **args, size_t smem_bytes,
+                               cudaStream_t stream) {
+  return launch_collective(func, grid_per_pe, block, args, smem_bytes, stream);
+}
+
+int nvshmemx_collective_max_ctas_per_pe(const void *func, int block_threads, size_t smem_bytes) {
+  return max_ctas_per_pe(func, block_threads, smem_bytes);
+}
+
+// -------------------------------------------------------------------- status
+int nvshmemx_status(void) {
+  Runtime &r = rt();
+  int code = r.host_err;
+  long long detail = r.host_detail;
+  r.host_err = 0;
+  r.host_detail = -1;
+  if (r.started) {
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+      if (code == 0) code = NVSHMEMX_ERR_CUDA;
+    } else {
+      int st[4] = {0, 0, 0, 0};
+      if (cudaMemcpy(st, r.d_status, sizeof st, cudaMemcpyDeviceToHost) == cudaSuccess && st[0] != 0) {
+        if (code == 0) {
+          code = st[0];
+          memcpy(&detail, st + 2, sizeof detail);
+        }
+        cudaMemset(r.d_status, 0, sizeof st);
+      }
+    }
+  }
+  r.last_detail = detail;
+  return code;
+}
+
+long long nvshmemx_status_detail(void) { return rt().last_detail; }
+
+void nvshmemx_set_error_mode(int mode) {
+  env_error_mode_read = true;
+  rt().error_mode = mode;
+}
+int nvshmemx_get_error_mode(void) {
+  read_env_error_mode();
+  return rt().error_mode;
+}
+
+const char *nvshmemx_strerror(int code) {
+  switch (code) {
+    case NVSHMEMX_SUCCESS: return "success";
+    case NVSHMEMX_ERR_INVALID: return "invalid argument";
+    case NVSHMEMX_ERR_NOMEM: return "out of symmetric heap or device memory";
+    case NVSHMEMX_ERR_CUDA: return "CUDA call failed";
+    case NVSHMEMX_ERR_STATE: return "library not started, already started, or a PE left";
+    case NVSHMEMX_ERR_TIMEOUT: return "wait or barrier deadline passed";
+    case NVSHMEMX_ERR_BOUNDS: return "access outside the symmetric arena (skipped)";
+    case NVSHMEMX_ERR_COOP: return "grid too large to be co-resident";
+    case NVSHMEMX_ERR_UNSUPPORTED: return "unsupported";
+    default: return "unknown";
+  }
+}
+
+// --------------------------------------------------------- arena and queries
+void *nvshmemx_arena_base(void) { return rt().arena; }
+size_t nvshmemx_slice_stride(void) { return rt().stride; }
+size_t nvshmemx_heap_size(void) { return rt().heap_bytes; }
+size_t nvshmemx_heap_used(int pe) {
+  Runtime &r = rt();
+  if (!r.started || pe < 0 || pe >= r.npes) return 0;
+  return r.tail[pe];
+}
+int nvshmemx_sm_count(void) {
+  Runtime &r = rt();
+  if (r.sm_count) return r.sm_count;
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n;
+}
+int nvshmemx_device_sync(void) { return check_cuda(cudaDeviceSynchronize(), "cudaDeviceSynchronize"); }
+
+static int heap_range_ok(int pe, size_t off, size_t bytes) {
+  Runtime &r = rt();
+  if (!r.started) return fail(NVSHMEMX_ERR_STATE, "heap access before nvstart_pes");
+  if (pe < 0 || pe >= r.npes || off > r.heap_bytes || bytes > r.heap_bytes - off)
+    return fail(NVSHMEMX_ERR_INVALID, "heap access pe %d [%zu, +%zu) outside the slice", pe, off, bytes);
+  return 0;
+}
+
+int nvshmemx_heap_write(int pe, size_t off, const void *src, size_t bytes) {
+  int rc = heap_range_ok(pe, off, bytes);
+  if (rc) return rc;
+  Runtime &r = rt();
+  return check_cuda(cudaMemcpy(r.arena + (size_t)pe * r.stride + off, src, bytes, cudaMemcpyHostToDevice),
+                    "cudaMemcpy(H2D)");
+}
+int nvshmemx_heap_read(int pe, size_t off, void *dst, size_t bytes) {
+  int rc = heap_range_ok(pe, off, bytes);
+  if (rc) return rc;
+  Runtime &r = rt();
+  return check_cuda(cudaMemcpy(dst, r.arena + (size_t)pe * r.stride + off, bytes, cudaMemcpyDeviceToHost),
+                    "cudaMemcpy(D2H)");
+}
+int nvshmemx_heap_memset(int pe, size_t off, int value, size_t bytes) {
+  int rc = heap_range_ok(pe, off, bytes);
+  if (rc) return rc;
+  Runtime &r = rt();
+  return check_cuda(cudaMemset(r.arena + (size_t)pe * r.stride + off, value, bytes), "cudaMemset");
+}
+
+void nvshmemx_set_wait_timeout_ns(long long ns) {
+  Runtime &r = rt();
+  r.wait_timeout_ns = ns > 0 ? ns : 5000000000LL;
+  if (r.started) {
+    r.cfg.wait_timeout_ns = r.wait_timeout_ns;
+    publish_cfg();
+  }
+}
+long long nvshmemx_get_wait_timeout_ns(void) { return rt().wait_timeout_ns; }
+
+// ------------------------------------------------------------- SPMD threads
+int nvshmemx_spmd_run(void (*fn)(void *), void *arg) {
+  Runtime &r = rt();
+  if (!r.started) return fail(NVSHMEMX_ERR_STATE, "nvshmemx_spmd_run before nvstart_pes");
+  if (r.spmd_active) return fail(NVSHMEMX_ERR_STATE, "nvshmemx_spmd_run: already running");
+  r.spmd_active = true;
+  g_hbar.n = r.npes;
+  g_hbar.count = 0;
+  g_hbar.departed = 0;
+  g_spmd_events.assign(r.npes, nullptr);
+  for (int p = 0; p < r.npes; ++p) cudaEventCreateWithFlags(&g_spmd_events[p], cudaEventDisableTiming);
+  std::vector<std::thread> th;
+  const int dev = r.device;
+  for (int p = 0; p < r.npes; ++p) {
+    th.emplace_back([=] {
+      cudaSetDevice(dev);
+      t_pe = p;
+      t_spmd = true;
+      fn(arg);
+      g_hbar.depart();
+      t_spmd = false;
+      t_pe = 0;
+    });
+  }
+  for (auto &t : th) t.join();
+  for (auto e : g_spmd_events) cudaEventDestroy(e);
+  g_spmd_events.clear();
+  r.spmd_active = false;
+  return r.host_err;
+}
+
+// ---------------------------------------------------------------- trace ring
+int nvshmemx_trace_enable(unsigned int records_per_pe) {
+  Runtime &r = rt();
+  std::lock_guard<std::recursive_mutex> lk(r.mu);
+  if (!r.started) return fail(NVSHMEMX_ERR_STATE, "trace before nvstart_pes");
+  unsigned cap = 1;
+  while (cap < records_per_pe) cap <<= 1;
+  if (cap < 16) cap = 16;
+  int rc;
+  cudaDeviceSynchronize();
+  if (r.d_trace) cudaFree(r.d_trace);
+  if (r.d_trace_head) cudaFree(r.d_trace_head);
+  r.d_trace = nullptr;
+  r.d_trace_head = nullptr;
+  if ((rc = check_cuda(cudaMalloc(&r.d_trace, (size_t)r.npes * cap * sizeof(nvshmemx_trace_record)),
+                       "cudaMalloc(trace)")))
+    return rc;
+  if ((rc = check_cuda(cudaMalloc(&r.d_trace_head, (size_t)r.npes * sizeof(unsigned long long)),
+                       "cudaMalloc(trace head)")))
+    return rc;
+  cudaMemset(r.d_trace, 0, (size_t)r.npes * cap * sizeof(nvshmemx_trace_record));
+  cudaMemset(r.d_trace_head, 0, (size_t)r.npes * sizeof(unsigned long long));
+  r.trace_cap = cap;
+  r.cfg.trace = r.d_trace;
+  r.cfg.trace_head = r.d_trace_head;
+  r.cfg.trace_cap = cap;
+  return publish_cfg();
+}
+
+int nvshmemx_trace_disable(void) {
+  Runtime &r = rt();
+  std::lock_guard<std::recursive_mutex> lk(r.mu);
+  if (!r.started) return fail(NVSHMEMX_ERR_STATE, "trace before nvstart_pes");
+  cudaDeviceSynchronize();
+  r.cfg.trace = nullptr;
+  r.cfg.trace_head = nullptr;
+  r.cfg.trace_cap = 0;
+  int rc = publish_cfg();
+  if (r.d_trace) cudaFree(r.d_trace);
+  if (r.d_trace_head) cudaFree(r.d_trace_head);
+  r.d_trace = nullptr;
+  r.d_trace_head = nullptr;
+  r.trace_cap = 0;
+  return rc;
+}
+
+int nvshmemx_trace_reset(void) {
+  Runtime &r = rt();
+  if (!r.d_trace_head) return fail(NVSHMEMX_ERR_STATE, "trace not enabled");
+  cudaDeviceSynchronize();
+  return check_cuda(cudaMemset(r.d_trace_head, 0, (size_t)r.npes * sizeof(unsigned long long)), "cudaMemset");
+}
+
+long long nvshmemx_trace_read(int pe, nvshmemx_trace_record *out, size_t max_records, long long *dropped) {
+  Runtime &r = rt();
+  if (!r.d_trace || pe < 0 || pe >= r.npes) return -1;
+  if (cudaDeviceSynchronize() != cudaSuccess) return -1;
+  unsigned long long head = 0;
+  if (cudaMemcpy(&head, r.d_trace_head + pe, sizeof head, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  unsigned long long n = head < r.trace_cap ? head : r.trace_cap;
+  unsigned long long first = head - n;  // oldest surviving record
+  if (dropped) *dropped = (long long)(head - n);
+  if (n > max_records) n = max_records;
+  std::vector<nvshmemx_trace_record> ring(r.trace_cap);
+  if (cudaMemcpy(ring.data(), r.d_trace + (size_t)pe * r.trace_cap, r.trace_cap * sizeof(nvshmemx_trace_record),
+                 cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  for (unsigned long long i = 0; i < n; ++i) out[i] = ring[(first + i) & (r.trace_cap - 1)];
+  return (long long)n;
+}
+
+// CSV layout of the prototype's processed trace files (nvshmem.cu:390 header,
+// :411-433 records): size is in elements for typed ops, 1 for p/g/wait.
+static const char *trace_op_name(int op) {
+  static const char *names[] = {"put_int", "put_float", "put_double", "get_int", "get_float",
+                                "get_double", "wait_int", "wait_until_int", "barrier", "quiet",
+                                "p", "g", "trace_begin", "trace_end"};
+  return (op >= 0 && op < 14) ? names[op] : "unknown";
+}
+
+int nvshmemx_trace_write_csv(const char *prefix) {
+  Runtime &r = rt();
+  if (!r.d_trace) return fail(NVSHMEMX_ERR_STATE, "trace not enabled");
+  std::string pre = prefix ? prefix : ("nvshmem_processed_tracefile_" + std::to_string((long)getpid()));
+  std::vector<nvshmemx_trace_record> recs(r.trace_cap);
+  for (int pe = 0; pe < r.npes; ++pe) {
+    long long dropped = 0;
+    long long n = nvshmemx_trace_read(pe, recs.data(), recs.size(), &dropped);
+    if (n < 0) return fail(NVSHMEMX_ERR_CUDA, "trace read failed");
+    std::string fn = pre + "_" + std::to_string(pe);
+    FILE *f = fopen(fn.c_str(), "w");
+    if (!f) return fail(NVSHMEMX_ERR_INVALID, "cannot open %s", fn.c_str());
+    fprintf(f, "# timestamp, gridid, blockid, tid, type, local_address, remote_address, size, remote_pe, timespent\n");
+    for (long long i = 0; i < n; ++i) {
+      const nvshmemx_trace_record &t = recs[i];
+      long long size = t.bytes;
+      if (t.op == NVSHMEMX_TRACE_PUT_DOUBLE || t.op == NVSHMEMX_TRACE_GET_DOUBLE)
+        size = t.bytes / 8;
+      else if (t.op <= NVSHMEMX_TRACE_GET_FLOAT)
+        size = t.bytes / 4;
+      else if (t.op == NVSHMEMX_TRACE_WAIT_INT || t.op == NVSHMEMX_TRACE_WAIT_UNTIL_INT)
+        size = 1;
+      fprintf(f, "%lld, %llu, %u, %u, %s, %p, %p, %lld, %u, %lld\n", t.t_ns, 0ull, t.block, (unsigned)t.tid,
+              trace_op_name(t.op), (void *)t.local_addr, (void *)t.remote_addr, size, (unsigned)t.peer,
+              t.spin_ns);
+    }
+    fclose(f);
+  }
+  return NVSHMEMX_SUCCESS;
+}
+
+}  // extern "C"

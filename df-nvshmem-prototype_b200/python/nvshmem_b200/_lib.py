@@ -1,0 +1,143 @@
+"""ctypes binding of libnvshmem_b200.so (the C ABI of include/nvshmemx_ops.h,
+include/nvshmemx_batch.h, include/nvshmemx.h and include/nvshmem.h).
+
+There is no fallback: if the shared library is missing this module raises at
+import, so nothing can silently run on the CPU instead of the GPU kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import (POINTER, c_char_p, c_double, c_float, c_int, c_longlong,
+                    c_size_t, c_uint, c_uint64, c_ulonglong, c_void_p)
+
+import numpy as np
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+LIB_PATH = os.environ.get("NVSHMEM_B200_LIB",
+                          os.path.join(PKG_ROOT, "lib", "libnvshmem_b200.so"))
+
+# status codes (include/nvshmemx.h)
+SUCCESS, ERR_INVALID, ERR_NOMEM, ERR_CUDA, ERR_STATE, ERR_TIMEOUT, ERR_BOUNDS, ERR_COOP, ERR_UNSUPPORTED = range(9)
+ERRORS_EXIT, ERRORS_RETURN = 0, 1
+CMP_EQ, CMP_NE, CMP_GT, CMP_GE, CMP_LT, CMP_LE = range(6)
+
+# requests (include/nvshmemx_ops.h)
+REQ_PUT, REQ_GET, REQ_SIGNAL, REQ_P, REQ_G = range(5)
+DT_INT, DT_FLOAT, DT_DOUBLE = range(3)
+DT_WIDTH = {DT_INT: 4, DT_FLOAT: 4, DT_DOUBLE: 8}
+MODE_THREAD, MODE_WARP, MODE_BLOCK, MODE_BULK = range(4)
+
+REQUEST_DTYPE = np.dtype([
+    ("src_off", "<u8"), ("dst_off", "<u8"), ("bytes", "<u4"),
+    ("src_pe", "<u2"), ("dst_pe", "<u2"), ("op", "u1"), ("dtype", "u1"),
+    ("flags", "<u2"), ("value", "<i4"),
+])
+assert REQUEST_DTYPE.itemsize == 32
+
+TRACE_DTYPE = np.dtype([
+    ("t_ns", "<i8"), ("spin_ns", "<i8"), ("local_addr", "<u8"), ("remote_addr", "<u8"),
+    ("bytes", "<u4"), ("op", "<u2"), ("pe", "<u2"), ("peer", "<u2"), ("tid", "<u2"),
+    ("block", "<u4"),
+])
+assert TRACE_DTYPE.itemsize == 48
+
+
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("vec_bytes", c_int), ("chunk_bytes", c_int), ("unroll", c_int),
+                ("threads", c_int), ("ctas_per_sm", c_int), ("grab", c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ShmemError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        super().__init__(f"{what}: {strerror(code)} ({code})")
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"native library {LIB_PATH} is missing: build it with "
+            f"`make -C {PKG_ROOT}` (or __graft_entry__.build())")
+    return ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL)
+
+
+lib = _load()
+
+_P = POINTER
+_SIGS = {
+    # nvshmem.h
+    "nvstart_pes": (None, []), "nvstop_pes": (None, []),
+    "nvshmem_my_pe": (c_int, []), "nvshmem_n_pes": (c_int, []),
+    "nvshmalloc": (c_void_p, [c_size_t]), "nvshmcleanup": (None, []),
+    "nvshmem_barrier_all": (None, []), "nvshmem_barrier_all_offload": (None, []),
+    "nvshmem_ptr": (c_void_p, [c_void_p, c_int]),
+    # nvshmemx.h host
+    "nvshmemx_init_attr": (c_int, [c_int, c_size_t]), "nvshmemx_finalize": (c_int, []),
+    "nvshmemx_is_started": (c_int, []), "nvshmemx_status": (c_int, []),
+    "nvshmemx_status_detail": (c_longlong, []),
+    "nvshmemx_set_error_mode": (None, [c_int]), "nvshmemx_get_error_mode": (c_int, []),
+    "nvshmemx_strerror": (c_char_p, [c_int]),
+    "nvshmemx_arena_base": (c_void_p, []), "nvshmemx_slice_stride": (c_size_t, []),
+    "nvshmemx_heap_size": (c_size_t, []), "nvshmemx_heap_used": (c_size_t, [c_int]),
+    "nvshmemx_heap_write": (c_int, [c_int, c_size_t, c_void_p, c_size_t]),
+    "nvshmemx_heap_read": (c_int, [c_int, c_size_t, c_void_p, c_size_t]),
+    "nvshmemx_heap_memset": (c_int, [c_int, c_size_t, c_int, c_size_t]),
+    "nvshmemx_sm_count": (c_int, []), "nvshmemx_device_sync": (c_int, []),
+    "nvshmemx_set_wait_timeout_ns": (None, [c_longlong]),
+    "nvshmemx_get_wait_timeout_ns": (c_longlong, []),
+    "nvshmemx_spmd_run": (c_int, [c_void_p, c_void_p]),
+    "nvshmemx_trace_enable": (c_int, [c_uint]), "nvshmemx_trace_disable": (c_int, []),
+    "nvshmemx_trace_read": (c_longlong, [c_int, c_void_p, c_size_t, _P(c_longlong)]),
+    "nvshmemx_trace_reset": (c_int, []), "nvshmemx_trace_write_csv": (c_int, [c_char_p]),
+    # nvshmemx_ops.h
+    "nvshmemx_exec_requests": (c_int, [c_void_p, c_int, c_int, _P(c_float)]),
+    "nvshmemx_fill_random": (c_int, [c_int, c_size_t, c_size_t, c_uint64]),
+    "nvshmemx_compare": (c_int, [c_int, c_size_t, c_int, c_size_t, c_size_t, _P(c_ulonglong)]),
+    "nvshmemx_checksum": (c_int, [c_int, c_size_t, c_size_t, _P(c_ulonglong)]),
+    "nvshmemx_op_pingpong": (c_int, [c_size_t, c_size_t, c_int, c_int, c_int, _P(c_double), _P(c_double)]),
+    "nvshmemx_op_barrier_latency": (c_int, [c_int, c_int, _P(c_double), _P(c_double)]),
+    "nvshmemx_op_offload_barrier": (c_int, [c_int, _P(c_double)]),
+    "nvshmemx_op_alltoall": (c_int, [c_int, c_int, c_size_t, c_size_t, c_size_t, c_int, c_int,
+                                     c_size_t, c_int, c_int, _P(c_float)]),
+    "nvshmemx_op_halo": (c_int, [c_int, c_int, c_int, c_int, c_size_t, c_size_t, c_size_t, c_int,
+                                 c_int, _P(c_float)]),
+    "nvshmemx_op_wait_test": (c_int, [c_size_t, c_int, c_longlong, _P(c_int)]),
+    "nvshmemx_op_barrier_fault_test": (c_int, [c_int, c_longlong, _P(c_int)]),
+    # nvshmemx_batch.h
+    "nvshmemx_batch_default_config": (None, [_P(BatchConfig)]),
+    "nvshmemx_batch_create": (c_int, [c_int, c_ulonglong, c_int, _P(c_void_p)]),
+    "nvshmemx_batch_destroy": (c_int, [c_void_p]),
+    "nvshmemx_batch_set_config": (c_int, [c_void_p, _P(BatchConfig)]),
+    "nvshmemx_batch_get_config": (c_int, [c_void_p, _P(BatchConfig)]),
+    "nvshmemx_batch_host_buffer": (c_void_p, [c_void_p]),
+    "nvshmemx_batch_upload": (c_int, [c_void_p, c_void_p, c_int]),
+    "nvshmemx_batch_execute": (c_int, [c_void_p, c_int, _P(c_float)]),
+    "nvshmemx_batch_submit": (c_int, [c_void_p, c_void_p, c_int, _P(c_int), _P(c_float)]),
+    "nvshmemx_batch_last_stats": (c_int, [c_void_p, _P(c_ulonglong), _P(c_float), _P(c_float)]),
+    "nvshmemx_requests_bytes": (c_ulonglong, [c_void_p, c_int]),
+    "nvshmemx_batch_execute_percall": (c_int, [c_void_p, c_int, c_int, _P(c_float)]),
+}
+
+for _name, (_res, _args) in _SIGS.items():
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+
+def strerror(code: int) -> str:
+    s = lib.nvshmemx_strerror(int(code))
+    return s.decode() if s else "unknown"
+
+
+def check(rc: int, what: str) -> None:
+    if rc != SUCCESS:
+        raise ShmemError(rc, what)
+
+
+def ptr(a: np.ndarray) -> int:
+    assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+    return a.ctypes.data

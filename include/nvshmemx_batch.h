@@ -1,0 +1,97 @@
+/*
+ * nvshmemx_batch.h -- batched one-sided traffic for the B200 virtual-PE
+ * library (plain C ABI).
+ *
+ * The prototype has no batching: every put/get is one call of the per-thread
+ * device API (nvshmem_device.cu:488-540) and the caller decides how many
+ * threads issue how many calls.  A batch here is an array of
+ * nvshmemx_request descriptors (nvshmemx_ops.h) that one CUDA graph executes
+ * with two kernels:
+ *   plan  -- validates and translates each request and cuts it into chunks of
+ *            at most chunk_bytes (a 0-byte SIGNAL/P is one chunk);
+ *   exec  -- a persistent grid whose warps claim chunks from a device-wide
+ *            cursor and copy them with coalesced vector accesses,
+ * so uneven request sizes and random PE pairs spread over every SM.  Results
+ * are bit-identical to issuing the same requests one by one (requests of one
+ * batch must not write bytes that another request of the batch reads or
+ * writes).
+ *
+ * How the copy is shaped (vector width, chunk size, accesses in flight,
+ * threads and CTAs per SM) is a nvshmemx_batch_config; the autotuner
+ * (nvshmemx_tune_batch) measures candidate configurations and keeps the best
+ * in a table, and the learned picker (nvshmemx_mlp_*) can predict it.
+ */
+#ifndef NVSHMEM_B200_NVSHMEMX_BATCH_H_
+#define NVSHMEM_B200_NVSHMEMX_BATCH_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "nvshmemx_ops.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct nvshmemx_batch_config {
+  int vec_bytes;    /* widest access: 4, 8 or 16                              */
+  int chunk_bytes;  /* work unit: multiple of 256 in [256, 1 MiB]             */
+  int unroll;       /* accesses in flight per lane: 1, 2, 4 or 8              */
+  int threads;      /* threads per CTA: 128, 256, 512 or 1024                 */
+  int ctas_per_sm;  /* resident CTAs per SM (0: as many as fit)               */
+  int grab;         /* chunks claimed per cursor atomic: 1..16                */
+} nvshmemx_batch_config;
+
+/* Sensible defaults for B200 (16-byte vectors, 16 KiB chunks, 4 in flight,
+ * 512 threads, 2 CTAs per SM, 2 chunks per claim). */
+void nvshmemx_batch_default_config(nvshmemx_batch_config *cfg);
+
+typedef struct nvshmemx_batch nvshmemx_batch;
+
+/* Device buffers for up to max_requests requests moving up to
+ * max_payload_bytes in total (sizes the chunk table for the smallest chunk
+ * size a configuration may use, 256 bytes, unless min_chunk_bytes is larger). */
+int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes, int min_chunk_bytes,
+                          nvshmemx_batch **out);
+int nvshmemx_batch_destroy(nvshmemx_batch *b);
+int nvshmemx_batch_set_config(nvshmemx_batch *b, const nvshmemx_batch_config *cfg);
+int nvshmemx_batch_get_config(const nvshmemx_batch *b, nvshmemx_batch_config *cfg);
+
+/* Pinned host staging buffer of max_requests descriptors owned by the batch;
+ * callers fill it and pass it to nvshmemx_batch_submit. */
+nvshmemx_request *nvshmemx_batch_host_buffer(nvshmemx_batch *b);
+
+/* Copies n requests to the device (synchronously) for later executions. */
+int nvshmemx_batch_upload(nvshmemx_batch *b, const nvshmemx_request *reqs, int n);
+
+/* Executes the uploaded requests `reps` times back to back (one graph launch
+ * each; the CUDA graph is rebuilt when n or the configuration changes).
+ * *out_ms receives the device time of all reps (CUDA events). */
+int nvshmemx_batch_execute(nvshmemx_batch *b, int reps, float *out_ms);
+
+/* End-to-end call: copies n requests from host memory (pinned if it is the
+ * batch's host buffer), executes them and reads back the batch status word,
+ * all on the batch's stream; *out_status receives the status (0 = every
+ * request done), *out_ms the device time of the whole sequence. */
+int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n, int *out_status,
+                          float *out_ms);
+
+/* Statistics of the last execution: chunk count and the kernel time of the
+ * exec kernel alone (CUDA events around it inside the last execution). */
+int nvshmemx_batch_last_stats(const nvshmemx_batch *b, unsigned long long *chunks, float *plan_ms,
+                              float *exec_ms);
+
+/* Algorithmic bytes of n requests: 2*bytes for PUT/GET (read + write),
+ * 2*width for G, 4 for SIGNAL, width for P. */
+unsigned long long nvshmemx_requests_bytes(const nvshmemx_request *reqs, int n);
+
+/* The per-call path on the same device-resident requests: one caller unit
+ * per request (mode NVSHMEMX_MODE_*) through the public device API, `reps`
+ * launches back to back; *out_ms the device time of all reps. */
+int nvshmemx_batch_execute_percall(nvshmemx_batch *b, int mode, int reps, float *out_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NVSHMEM_B200_NVSHMEMX_BATCH_H_ */

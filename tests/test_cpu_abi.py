@@ -1,0 +1,110 @@
+"""The C ABI without a GPU: the shared library loads, exports every host
+function include/*.h declares, and the status/error paths that need no device
+behave as documented (error return vs the prototype's exit(-1)).  Device
+functions of nvshmem_device.h / nvshmemx.h are checked by linking a program
+that calls each of them against the static library."""
+import ctypes
+import os
+import re
+import subprocess
+import sys
+
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+INC = os.path.join(REPO, "include")
+PKG = os.path.join(REPO, "df-nvshmem-prototype_b200")
+
+DECL = re.compile(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(nvshm\w+|nvstart_pes|nvstop_pes)\s*\(", re.M)
+
+
+def declared(device: bool):
+    names = set()
+    for h in sorted(os.listdir(INC)):
+        text = open(os.path.join(INC, h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for line in text.splitlines():
+            if "#define" in line or "typedef" in line:
+                continue
+            m = DECL.match(line)
+            if not m:
+                continue
+            is_dev = "__device__" in line
+            if is_dev == device:
+                names.add(m.group(1))
+    return names
+
+
+def test_shared_library_exports_every_host_symbol():
+    from nvshmem_b200._lib import LIB_PATH
+    lib = ctypes.CDLL(LIB_PATH)
+    names = declared(device=False)
+    assert len(names) > 50
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_device_symbols_declared():
+    names = declared(device=True)
+    for n in ("nvshmem_int_put", "nvshmem_double_get", "nvshmem_int_wait_until", "nvshmem_quiet",
+              "nvshmem_float_p", "nvshmem_double_g", "nvshmemx_barrier_all", "nvshmemx_putmem_bulk_block"):
+        assert n in names
+
+
+def _run(code: str, env=None):
+    return subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120,
+                          env=env, cwd=REPO)
+
+
+PRE = ("import sys; sys.path.insert(0, %r); from nvshmem_b200 import _lib as L; lib = L.lib\n"
+       % os.path.join(PKG, "python"))
+
+
+def test_error_mode_exit_matches_prototype():
+    # nvshmalloc before start: the prototype prints and calls exit(-1)
+    r = _run(PRE + "lib.nvshmalloc(16)\nprint('not reached')")
+    assert r.returncode == 255 and "not reached" not in r.stdout
+    assert "nvshmalloc before nvstart_pes" in r.stderr
+
+
+def test_error_mode_return():
+    r = _run(PRE + "lib.nvshmemx_set_error_mode(L.ERRORS_RETURN)\n"
+             "p = lib.nvshmalloc(16)\nprint(p, lib.nvshmemx_status(), lib.nvshmemx_status())")
+    assert r.returncode == 0, r.stderr
+    p, st1, st2 = r.stdout.split()
+    assert p == "None" and int(st1) == 4 and int(st2) == 0  # ERR_STATE once, then cleared
+
+
+def test_error_mode_from_environment():
+    env = dict(os.environ, NVSHMEM_ERROR_MODE="return")
+    r = _run(PRE + "print(lib.nvshmemx_get_error_mode(), lib.nvshmem_ptr(None, 0))", env=env)
+    assert r.stdout.split()[0] == "1"
+
+
+def test_strerror_and_queries_without_start():
+    from nvshmem_b200._lib import lib, strerror
+    assert strerror(5) == "wait or barrier deadline passed"
+    assert lib.nvshmemx_is_started() == 0
+    assert lib.nvshmem_n_pes() == 0 and lib.nvshmem_my_pe() == 0
+
+
+def test_bad_init_arguments_return_codes():
+    r = _run(PRE + "lib.nvshmemx_set_error_mode(1)\n"
+             "print(lib.nvshmemx_init_attr(0, 1<<20), lib.nvshmemx_init_attr(5000, 1<<20), "
+             "lib.nvshmemx_init_attr(2, 0))")
+    assert r.stdout.split() == ["1", "1", "1"]
+
+
+NATIVE = os.path.join(REPO, "tests", "native")
+
+
+@pytest.mark.skipif(subprocess.run(["which", "nvcc"], capture_output=True).returncode != 0, reason="no nvcc")
+def test_every_device_function_links_against_static_lib(tmp_path):
+    src = os.path.join(NATIVE, "api_all.cu")
+    out = tmp_path / "api_all"
+    lib = os.path.join(PKG, "lib")
+    r = subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-rdc=true", "-I", INC, src,
+                        "-o", str(out), "-L", lib, "-lnvshmem", "-L/usr/local/cuda/lib64/stubs", "-lcuda"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-3000:]
+    assert out.exists()

@@ -1,0 +1,126 @@
+"""Parity of the batched engine against the CPU oracle and against the
+per-call path: uneven request batches (C4 traffic) must leave every heap
+bit-identical whatever the batch configuration, at small sizes byte for byte
+and at the full 64-PE x 64 MiB size through per-PE checksums."""
+import numpy as np
+import pytest
+
+from nvshmem_b200 import (ERR_BOUNDS, MODE_THREAD, MODE_WARP, REQ_PUT,
+                          requests_bytes)
+from nvshmem_b200.traffic import c4_batch, check_disjoint
+from oracle.model import Model, checksum
+from _util import first_diff, heap_images, random_requests, requests
+
+pytestmark = pytest.mark.gpu
+
+CONFIGS = [
+    dict(vec_bytes=16, chunk_bytes=16384, unroll=4, threads=512, ctas_per_sm=2, grab=2),
+    dict(vec_bytes=16, chunk_bytes=256, unroll=1, threads=128, ctas_per_sm=1, grab=1),
+    dict(vec_bytes=8, chunk_bytes=4096, unroll=8, threads=1024, ctas_per_sm=0, grab=16),
+    dict(vec_bytes=4, chunk_bytes=65536, unroll=2, threads=256, ctas_per_sm=4, grab=4),
+]
+
+
+def setup(shmem_factory, npes, heap, seed=7):
+    sh = shmem_factory(npes, heap)
+    om = Model(npes, heap)
+    for pe in range(npes):
+        sh.fill_random(pe, 0, heap, seed)
+        om.fill_random(pe, 0, heap, seed)
+    return sh, om
+
+
+@pytest.mark.parametrize("cfg", CONFIGS)
+def test_c4_small_bit_exact(shmem_factory, cfg):
+    npes, heap = 16, 4 << 20
+    reqs = c4_batch(seed=4, n=3000, npes=npes, heap=heap, hi=256 << 10)
+    assert check_disjoint(reqs)
+    sh, om = setup(shmem_factory, npes, heap)
+    with sh.batch(len(reqs), int(reqs["bytes"].sum()), 256) as b:
+        b.set_config(cfg)
+        b.upload(reqs)
+        b.execute(1)
+        b.execute(2)  # idempotent: sources never overlap destinations
+        chunks, _, _ = b.stats()
+        assert chunks >= len(reqs) - np.count_nonzero(reqs["bytes"] == 0) // 2
+    assert sh.status() == 0
+    om.apply_requests(reqs)
+    assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+
+
+def test_mixed_ops_and_alignments(shmem_factory):
+    npes, heap = 8, 2 << 20
+    reqs = random_requests(77, 800, npes, heap, max_bytes=40000)
+    sh, om = setup(shmem_factory, npes, heap)
+    with sh.batch(len(reqs), int(reqs["bytes"].sum()) + 8 * len(reqs), 256) as b:
+        b.set_config(dict(vec_bytes=16, chunk_bytes=1024, unroll=4, threads=256, ctas_per_sm=2, grab=2))
+        b.upload(reqs)
+        b.execute(1)
+    assert sh.status() == 0
+    om.apply_requests(reqs)
+    assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+
+
+@pytest.mark.parametrize("mode", [MODE_THREAD, MODE_WARP])
+def test_percall_equals_batch(shmem_factory, mode):
+    npes, heap = 8, 4 << 20
+    reqs = c4_batch(seed=9, n=2000, npes=npes, heap=heap, hi=128 << 10)
+    sh, om = setup(shmem_factory, npes, heap)
+    with sh.batch(len(reqs), int(reqs["bytes"].sum()), 4096) as b:
+        b.upload(reqs)
+        b.percall(mode, 1)
+        assert sh.status() == 0
+        om.apply_requests(reqs)
+        assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+        b.execute(1)
+        assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+
+
+def test_submit_end_to_end(shmem_factory):
+    npes, heap = 8, 4 << 20
+    reqs = c4_batch(seed=10, n=2000, npes=npes, heap=heap, hi=128 << 10)
+    sh, om = setup(shmem_factory, npes, heap)
+    with sh.batch(len(reqs), int(reqs["bytes"].sum()), 4096) as b:
+        buf = b.host_buffer()
+        buf[:len(reqs)] = reqs
+        st, ms = b.submit(buf, len(reqs))
+        assert st == 0 and ms > 0
+    om.apply_requests(reqs)
+    assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+
+
+def test_bad_request_rejected_not_executed(shmem_factory):
+    npes, heap = 4, 1 << 20
+    sh, om = setup(shmem_factory, npes, heap)
+    reqs = requests([dict(src_off=0, dst_off=heap - 16, bytes=64, src_pe=0, dst_pe=1, op=REQ_PUT, dtype=0),
+                     dict(src_off=0, dst_off=heap // 2, bytes=64, src_pe=0, dst_pe=9, op=REQ_PUT, dtype=0)])
+    with sh.batch(4, 1 << 16, 256) as b:
+        b.upload(reqs)
+        with pytest.raises(Exception):
+            b.execute(1)
+    sh.status()
+    assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+
+
+def test_empty_batch(shmem_factory):
+    sh = shmem_factory(2, 1 << 20)
+    with sh.batch(16, 1 << 16, 256) as b:
+        b.upload(requests([]))
+        b.execute(3)
+    assert sh.status() == 0
+
+
+def test_c4_full_size_checksums(shmem_factory):
+    """The benchmark's batch: 64 PEs x 64 MiB, 100,000 requests."""
+    npes, heap = 64, 64 << 20
+    reqs = c4_batch(seed=4, n=100_000, npes=npes, heap=heap)
+    assert check_disjoint(reqs)
+    sh, om = setup(shmem_factory, npes, heap, seed=44)
+    with sh.batch(len(reqs), int(reqs["bytes"].sum()), 4096) as b:
+        b.upload(reqs)
+        b.execute(3)
+    assert sh.status() == 0
+    om.apply_requests(reqs)
+    for pe in range(npes):
+        assert sh.checksum(pe, 0, heap) == checksum(om.heap[pe]), f"PE {pe}"
+    assert requests_bytes(reqs) > 0

@@ -1,0 +1,146 @@
+"""Parity of the collective-launch patterns against the CPU oracle: the C1
+ping-pong, C2 all-to-all rounds (every mode, put and get, every element type,
+sizes from 8 B up) and the C3 halo exchange; plus the bounded-wait and
+barrier failure paths, which must end with NVSHMEMX_ERR_TIMEOUT, never hang."""
+import numpy as np
+import pytest
+
+from nvshmem_b200 import (DT_DOUBLE, DT_FLOAT, DT_INT, ERR_TIMEOUT, MODE_BLOCK,
+                          MODE_BULK, MODE_THREAD, MODE_WARP, REQ_GET, REQ_PUT)
+from nvshmem_b200.traffic import c3_block
+from oracle.model import Model
+from _util import first_diff, heap_images
+
+pytestmark = pytest.mark.gpu
+
+
+def test_pingpong_flags_and_data(shmem_factory):
+    heap = 1 << 20
+    sh = shmem_factory(2, heap)
+    om = Model(2, heap)
+    flag = sh.alloc(4)
+    data = sh.alloc(4096 * 4)
+    assert (flag, data) == (om.alloc(4), om.alloc(4096 * 4))
+    for pe in range(2):
+        sh.fill_random(pe, data, 4096 * 4, 5)
+        om.fill_random(pe, data, 4096 * 4, 5)
+    iters, skip = 1000, 20
+    ns, total = sh.pingpong(flag, data, 4096, iters, skip)
+    assert sh.status() == 0
+    om.pingpong(flag, data, 4096, iters + skip)
+    assert first_diff(heap_images(sh, 2, heap), om.heap) is None
+    assert total > 0 and np.all(ns > 0)
+
+
+def test_pingpong_flag_only_latency(shmem_factory):
+    sh = shmem_factory(2, 1 << 20)
+    flag = sh.alloc(4)
+    ns, total = sh.pingpong(flag, 0, 0, 10000, 20)
+    assert sh.status() == 0
+    assert sh.read(0, flag, 4, np.int32)[0] == 10020
+    assert sh.read(1, flag, 4, np.int32)[0] == 10020
+    p50 = float(np.median(ns))
+    assert 0 < p50 < 50_000  # a round trip through L2, far below 50 us
+
+
+@pytest.mark.parametrize("ctas", [1, 4])
+def test_barrier_latency(shmem_factory, ctas):
+    sh = shmem_factory(8, 1 << 20)
+    ns, total = sh.barrier_latency(ctas, 2000)
+    assert sh.status() == 0
+    assert 0 < np.median(ns) < 100_000
+
+
+def test_offload_barrier(shmem_factory):
+    sh = shmem_factory(8, 1 << 20)
+    us = sh.offload_barrier(200)
+    assert sh.status() == 0 and us > 0
+
+
+@pytest.mark.parametrize("mode", [MODE_THREAD, MODE_WARP, MODE_BLOCK, MODE_BULK])
+@pytest.mark.parametrize("op", [REQ_PUT, REQ_GET])
+def test_alltoall_small_sizes(shmem_factory, mode, op):
+    npes, heap = 8, 4 << 20
+    sh = shmem_factory(npes, heap)
+    om = Model(npes, heap)
+    for pe in range(npes):
+        sh.fill_random(pe, 0, heap, 1)
+        om.fill_random(pe, 0, heap, 1)
+    for dtype, nbytes in [(DT_INT, 8), (DT_FLOAT, 4100), (DT_DOUBLE, 65536), (DT_INT, 123456)]:
+        send, recv = 0, heap // 2
+        sh.alltoall(op, dtype, send, recv, nbytes, rounds=2, mode=mode, ctas_per_pe=3)
+        assert sh.status() == 0
+        om.alltoall(1 if op == REQ_GET else 0, send, recv, nbytes, rounds=2)
+    assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+
+
+def test_alltoall_rotating_sets(shmem_factory):
+    npes, heap = 8, 8 << 20
+    sh = shmem_factory(npes, heap)
+    om = Model(npes, heap)
+    for pe in range(npes):
+        sh.fill_random(pe, 0, heap, 9)
+        om.fill_random(pe, 0, heap, 9)
+    nbytes, stride = 65536, 1 << 20
+    sh.alltoall(REQ_PUT, DT_FLOAT, 0, 4 << 20, nbytes, rounds=5, nsets=3, set_stride=stride,
+                mode=MODE_BULK, ctas_per_pe=4)
+    om.alltoall(0, 0, 4 << 20, nbytes, rounds=5, nsets=3, set_stride=stride)
+    assert sh.status() == 0
+    assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+
+
+def test_alltoall_large_on_device_compare(shmem_factory):
+    """64 MiB messages: every received block equals the sender's block."""
+    npes, nbytes = 8, 64 << 20
+    heap = 2 * npes * nbytes
+    sh = shmem_factory(npes, heap)
+    for pe in range(npes):
+        sh.fill_random(pe, 0, npes * nbytes, 21)
+        sh.memset(pe, npes * nbytes, 0, npes * nbytes)
+    sh.alltoall(REQ_PUT, DT_DOUBLE, 0, npes * nbytes, nbytes, mode=MODE_BLOCK, ctas_per_pe=18)
+    assert sh.status() == 0
+    for p in range(npes):
+        for q in range(npes):
+            if p == q:
+                continue
+            assert sh.compare(q, npes * nbytes + p * nbytes, p, q * nbytes, nbytes) == 0
+
+
+@pytest.mark.parametrize("n", [8, 32])
+def test_halo_bit_exact(shmem_factory, n):
+    npes = 8
+    block = n * n * n * 8
+    heap = block + 6 * n * n * 8 + 4096
+    heap = (heap + 4095) // 4096 * 4096
+    sh = shmem_factory(npes, heap)
+    om = Model(npes, heap)
+    block_off, ghost_off, sig_off = 0, block, block + 6 * n * n * 8
+    for pe in range(npes):
+        b = c3_block(n, pe)
+        sh.write(pe, block_off, b)
+        om.heap[pe, block_off:block_off + block] = b.view(np.uint8)
+    sh.halo(2, 2, 2, n, block_off, ghost_off, sig_off, iters=5, ctas_per_pe=4)
+    assert sh.status() == 0
+    om.halo(2, 2, 2, n, block_off, ghost_off, sig_off, 5)
+    assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+
+
+def test_wait_timeout_reports_and_returns(shmem_factory):
+    sh = shmem_factory(2, 1 << 20)
+    flag = sh.alloc(4)
+    st = sh.wait_test(flag, 12345, 2_000_000)  # 2 ms, nothing ever sets it
+    assert st == ERR_TIMEOUT
+    assert sh.status() == ERR_TIMEOUT
+    sh.write(0, flag, np.array([12345], np.int32))
+    assert sh.wait_test(flag, 12345, 2_000_000) == 0
+    assert sh.status() == 0
+
+
+def test_barrier_with_missing_pe_times_out(shmem_factory):
+    sh = shmem_factory(4, 1 << 20)
+    st = sh.barrier_fault_test(2, 5_000_000)
+    assert st == ERR_TIMEOUT
+    assert sh.status() == ERR_TIMEOUT
+    # the context is still usable afterwards
+    ns, _ = sh.barrier_latency(1, 100)
+    assert sh.status() == 0

@@ -1,0 +1,101 @@
+"""Parity of the one-sided device API (p/g/put/get/signal) against the CPU
+oracle: request lists executed through nvshmem_{int,float,double}_{p,g,put,get}
+and the warp / block / TMA-bulk cooperative forms must leave heap images
+bit-identical to the oracle's."""
+import numpy as np
+import pytest
+
+from nvshmem_b200 import (DT_DOUBLE, DT_FLOAT, DT_INT, ERR_BOUNDS, MODE_BLOCK,
+                          MODE_BULK, MODE_THREAD, MODE_WARP, REQ_G, REQ_GET,
+                          REQ_P, REQ_PUT, REQ_SIGNAL)
+from oracle.model import Model
+from _util import first_diff, heap_images, random_requests, requests
+
+pytestmark = pytest.mark.gpu
+
+HEAP = 1 << 20
+MODES = [MODE_THREAD, MODE_WARP, MODE_BLOCK, MODE_BULK]
+
+
+def start(shmem_factory, npes, heap=HEAP, seed=11):
+    sh = shmem_factory(npes, heap)
+    om = Model(npes, heap)
+    for pe in range(npes):
+        sh.fill_random(pe, 0, heap, seed)
+        om.fill_random(pe, 0, heap, seed)
+    return sh, om
+
+
+def test_fill_matches_oracle(shmem_factory):
+    sh, om = start(shmem_factory, 3, seed=123)
+    got = heap_images(sh, 3, HEAP)
+    assert first_diff(got, om.heap) is None
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_random_requests_bit_exact(shmem_factory, mode):
+    npes = 4
+    sh, om = start(shmem_factory, npes)
+    reqs = random_requests(100 + mode, 300, npes, HEAP, max_bytes=20000)
+    sh.exec_requests(reqs, mode)
+    assert sh.status() == 0
+    om.apply_requests(reqs)
+    got = heap_images(sh, npes, HEAP)
+    assert first_diff(got, om.heap) is None
+
+
+@pytest.mark.parametrize("dtype", [DT_INT, DT_FLOAT, DT_DOUBLE])
+@pytest.mark.parametrize("nelems", [0, 1, 2, 3, 5, 31, 32, 33, 257, 4099, 65536])
+def test_put_get_lengths(shmem_factory, dtype, nelems):
+    """Every length, including 0 and lengths that leave ragged heads/tails."""
+    w = 8 if dtype == DT_DOUBLE else 4
+    sh, om = start(shmem_factory, 2)
+    rows = [dict(src_off=64 + 4, dst_off=HEAP // 2 + 8, bytes=nelems * w, src_pe=0, dst_pe=1,
+                 op=REQ_PUT, dtype=dtype),
+            dict(src_off=128, dst_off=HEAP // 2 + 200000 + 4 * (w == 4), bytes=nelems * w, src_pe=1,
+                 dst_pe=0, op=REQ_GET, dtype=dtype)]
+    reqs = requests(rows)
+    for mode in MODES:
+        sh.exec_requests(reqs, mode)
+        assert sh.status() == 0
+    om.apply_requests(reqs)
+    assert first_diff(heap_images(sh, 2, HEAP), om.heap) is None
+
+
+def test_p_g_all_types(shmem_factory):
+    sh, om = start(shmem_factory, 2)
+    rows = []
+    for i, dt in enumerate([DT_INT, DT_FLOAT, DT_DOUBLE] * 4):
+        bits = (0x7FF8000000000001 if dt == DT_DOUBLE else 0x7FC00001) + i  # NaN payloads too
+        rows.append(dict(src_off=bits, dst_off=HEAP // 2 + 16 * i, bytes=0, src_pe=i % 2, dst_pe=(i + 1) % 2,
+                         op=REQ_P, dtype=dt))
+        rows.append(dict(src_off=1024 + 16 * i, dst_off=HEAP // 2 + 4096 + 16 * i, bytes=0, src_pe=(i + 1) % 2,
+                         dst_pe=i % 2, op=REQ_G, dtype=dt))
+    reqs = requests(rows)
+    sh.exec_requests(reqs, MODE_THREAD)
+    assert sh.status() == 0
+    om.apply_requests(reqs)
+    assert first_diff(heap_images(sh, 2, HEAP), om.heap) is None
+
+
+def test_out_of_bounds_is_skipped_and_reported(shmem_factory):
+    sh, om = start(shmem_factory, 2)
+    bad = requests([dict(src_off=0, dst_off=HEAP - 8, bytes=64, src_pe=0, dst_pe=1, op=REQ_PUT, dtype=DT_INT),
+                    dict(src_off=0, dst_off=HEAP // 2 + 2, bytes=0, src_pe=0, dst_pe=1, op=REQ_SIGNAL,
+                         dtype=DT_INT, value=7)])
+    for mode in (MODE_THREAD, MODE_WARP, MODE_BLOCK):
+        sh.exec_requests(bad, mode)
+        assert sh.status() == ERR_BOUNDS
+    # nothing was written
+    assert first_diff(heap_images(sh, 2, HEAP), om.heap) is None
+
+
+def test_signal_values(shmem_factory):
+    sh, om = start(shmem_factory, 3)
+    rows = [dict(src_off=0, dst_off=HEAP // 2 + 4 * i, bytes=0, src_pe=i % 3, dst_pe=(i + 1) % 3, op=REQ_SIGNAL,
+                 dtype=DT_INT, value=-5 + 1000 * i) for i in range(64)]
+    reqs = requests(rows)
+    sh.exec_requests(reqs, MODE_WARP)
+    om.apply_requests(reqs)
+    assert sh.status() == 0
+    assert first_diff(heap_images(sh, 3, HEAP), om.heap) is None
