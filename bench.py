@@ -84,7 +84,7 @@ class ClockSampler:
         sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]})
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
         load = sorted(sm)[len(sm) // 2:] if sm else []
         return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
@@ -211,15 +211,19 @@ def run_gpu(args, rank, world, local):
                 # device-resident batches: K steps, L2 flushed between steps
                 torch.cuda.synchronize()
                 barrier(dist)
-                step_ms, exec_ms = [], []
+                step_ms = []
                 for _ in range(args.steps):
                     flush()
                     step_ms.append(b.execute(1))
-                    exec_ms.append(b.stats()[2])
                 torch.cuda.synchronize()
                 barrier(dist)
                 t_batch = reduce_max(dist, sum(step_ms) / 1e3)
                 chunks = b.stats()[0]
+                # the exec kernel alone (CUDA events around it on its stream)
+                exec_ms = []
+                for _ in range(args.steps):
+                    flush()
+                    exec_ms.append(b.execute_direct(1)[1])
                 # per-call path on the same batch (one thread per request)
                 pc = {}
                 for mode, name in ((MODE_THREAD, "thread"), (MODE_WARP, "warp")):

@@ -233,7 +233,7 @@ struct nvshmemx_batch {
   nvshmemx_batch_config graph_cfg{};
   Cfg graph_arena{};
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr, ev_plan0 = nullptr, ev_exec0 = nullptr, ev_exec1 = nullptr;
-  bool timed_graph = false;
+  bool timed_direct = false;  // ev_plan0/ev_exec0/ev_exec1 hold the last direct execution
 };
 
 static void drop_graph(nvshmemx_batch *b) {
@@ -252,6 +252,7 @@ static int enqueue_batch(nvshmemx_batch *b, bool with_events) {
   const nvshmemx_batch_config &k = b->cfg;
   ExecFn fn = pick_exec(k.vec_bytes, k.unroll);
   if (!fn) return fail(NVSHMEMX_ERR_INVALID, "batch: no kernel for vec %d unroll %d", k.vec_bytes, k.unroll);
+  (void)cudaGetLastError();  // report only this enqueue's own launch errors
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, k.threads, 0);
   if (per_sm < 1) per_sm = 1;
@@ -276,7 +277,7 @@ static int ensure_graph(nvshmemx_batch *b) {
   int rc;
   if ((rc = check_cuda(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture")))
     return rc;
-  int erc = enqueue_batch(b, true);
+  int erc = enqueue_batch(b, false);
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaStreamEndCapture(b->stream, &g);
   if (erc) {
@@ -394,7 +395,6 @@ int nvshmemx_batch_execute(nvshmemx_batch *b, int reps, float *out_ms) {
   float ms = 0;
   cudaEventElapsedTime(&ms, b->ev_start, b->ev_stop);
   if (out_ms) *out_ms = ms;
-  b->timed_graph = true;
   int st[2] = {0, 0};
   cudaMemcpy(st, &b->d_ctl->status, sizeof st, cudaMemcpyDeviceToHost);
   if (st[0]) return fail(st[0], "batch_execute: request %d rejected (%s)", st[1], nvshmemx_strerror(st[0]));
@@ -422,7 +422,6 @@ int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n
   cudaEventElapsedTime(&ms, b->ev_start, b->ev_stop);
   if (out_ms) *out_ms = ms;
   if (out_status) *out_status = b->h_status[0];
-  b->timed_graph = true;
   return 0;
 }
 
@@ -430,16 +429,45 @@ int nvshmemx_batch_last_stats(const nvshmemx_batch *b, unsigned long long *chunk
   if (!b) return NVSHMEMX_ERR_INVALID;
   if (chunks) {
     BatchCtl h;
-    cudaMemcpy(&h, b->d_ctl, sizeof h, cudaMemcpyDeviceToHost);
+    if (cudaMemcpy(&h, b->d_ctl, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return check_cuda(cudaGetLastError(), "batch_last_stats");
     *chunks = h.total_chunks;
   }
-  if (b->timed_graph) {
-    float p = 0, e = 0;
+  float p = 0, e = 0;
+  if (b->timed_direct) {
     cudaEventElapsedTime(&p, b->ev_plan0, b->ev_exec0);
     cudaEventElapsedTime(&e, b->ev_exec0, b->ev_exec1);
-    if (plan_ms) *plan_ms = p;
-    if (exec_ms) *exec_ms = e;
   }
+  if (plan_ms) *plan_ms = p;
+  if (exec_ms) *exec_ms = e;
+  return 0;
+}
+
+// Same work as one graph launch, enqueued directly with CUDA events around
+// the plan and exec kernels on the batch's stream, so the exec kernel's own
+// duration can be read (events recorded inside a captured graph are not used
+// for timing).  *out_exec_ms sums the exec kernel over all reps.
+int nvshmemx_batch_execute_direct(nvshmemx_batch *b, int reps, float *out_ms, float *out_exec_ms) {
+  if (!b || reps < 1) return fail(NVSHMEMX_ERR_INVALID, "batch_execute_direct: bad arguments");
+  int rc;
+  float total = 0, exec = 0;
+  for (int i = 0; i < reps; ++i) {
+    cudaEventRecord(b->ev_start, b->stream);
+    if ((rc = enqueue_batch(b, true))) return rc;
+    cudaEventRecord(b->ev_stop, b->stream);
+    if ((rc = check_cuda(cudaStreamSynchronize(b->stream), "batch_execute_direct"))) return rc;
+    float t = 0, e = 0;
+    cudaEventElapsedTime(&t, b->ev_start, b->ev_stop);
+    cudaEventElapsedTime(&e, b->ev_exec0, b->ev_exec1);
+    total += t;
+    exec += e;
+  }
+  b->timed_direct = true;
+  if (out_ms) *out_ms = total;
+  if (out_exec_ms) *out_exec_ms = exec;
+  int st[2] = {0, 0};
+  cudaMemcpy(st, &b->d_ctl->status, sizeof st, cudaMemcpyDeviceToHost);
+  if (st[0]) return fail(st[0], "batch_execute_direct: request %d rejected (%s)", st[1], nvshmemx_strerror(st[0]));
   return 0;
 }
 

@@ -412,6 +412,10 @@ using namespace nvshm;
 
 static int need_started() {
   if (!is_started()) return fail(NVSHMEMX_ERR_STATE, "operation before nvstart_pes");
+  // Drop a non-sticky error left by an earlier, unrelated runtime call so the
+  // launch checks below report only this operation's own failures (sticky
+  // device errors persist and are still reported).
+  (void)cudaGetLastError();
   return 0;
 }
 

@@ -49,6 +49,8 @@ static void read_env_error_mode() {
   if (m && strcmp(m, "return") == 0) rt().error_mode = NVSHMEMX_ERRORS_RETURN;
 }
 
+static char g_last_msg[512];
+
 int fail(int code, const char *fmt, ...) {
   Runtime &r = rt();
   read_env_error_mode();
@@ -57,6 +59,7 @@ int fail(int code, const char *fmt, ...) {
   va_start(ap, fmt);
   vsnprintf(msg, sizeof msg, fmt, ap);
   va_end(ap);
+  memcpy(g_last_msg, msg, sizeof msg);
   if (r.host_err == 0) r.host_err = code;
   if (r.error_mode == NVSHMEMX_ERRORS_EXIT) {
     fprintf(stderr, "[nvshmem %d] %s\n", t_pe, msg);
@@ -542,6 +545,8 @@ int nvshmemx_status(void) {
 }
 
 long long nvshmemx_status_detail(void) { return rt().last_detail; }
+
+const char *nvshmemx_last_error_string(void) { return nvshm::g_last_msg; }
 
 void nvshmemx_set_error_mode(int mode) {
   env_error_mode_read = true;

@@ -54,7 +54,9 @@ class BatchConfig(ctypes.Structure):
 class ShmemError(RuntimeError):
     def __init__(self, code: int, what: str):
         self.code = code
-        super().__init__(f"{what}: {strerror(code)} ({code})")
+        detail = lib.nvshmemx_last_error_string()
+        detail = detail.decode(errors="replace") if detail else ""
+        super().__init__(f"{what}: {strerror(code)} ({code}) {detail}")
 
 
 def _load():
@@ -81,6 +83,7 @@ _SIGS = {
     "nvshmemx_status_detail": (c_longlong, []),
     "nvshmemx_set_error_mode": (None, [c_int]), "nvshmemx_get_error_mode": (c_int, []),
     "nvshmemx_strerror": (c_char_p, [c_int]),
+    "nvshmemx_last_error_string": (c_char_p, []),
     "nvshmemx_arena_base": (c_void_p, []), "nvshmemx_slice_stride": (c_size_t, []),
     "nvshmemx_heap_size": (c_size_t, []), "nvshmemx_heap_used": (c_size_t, [c_int]),
     "nvshmemx_heap_write": (c_int, [c_int, c_size_t, c_void_p, c_size_t]),
@@ -116,6 +119,7 @@ _SIGS = {
     "nvshmemx_batch_host_buffer": (c_void_p, [c_void_p]),
     "nvshmemx_batch_upload": (c_int, [c_void_p, c_void_p, c_int]),
     "nvshmemx_batch_execute": (c_int, [c_void_p, c_int, _P(c_float)]),
+    "nvshmemx_batch_execute_direct": (c_int, [c_void_p, c_int, _P(c_float), _P(c_float)]),
     "nvshmemx_batch_submit": (c_int, [c_void_p, c_void_p, c_int, _P(c_int), _P(c_float)]),
     "nvshmemx_batch_last_stats": (c_int, [c_void_p, _P(c_ulonglong), _P(c_float), _P(c_float)]),
     "nvshmemx_requests_bytes": (c_ulonglong, [c_void_p, c_int]),

@@ -219,6 +219,12 @@ class Batch:
         check(lib.nvshmemx_batch_execute(self.h, reps, byref(ms)), "batch_execute")
         return ms.value
 
+    def execute_direct(self, reps: int = 1):
+        """(total ms, exec-kernel ms) of `reps` executions without the graph."""
+        ms, ex = c_float(0), c_float(0)
+        check(lib.nvshmemx_batch_execute_direct(self.h, reps, byref(ms), byref(ex)), "batch_execute_direct")
+        return ms.value, ex.value
+
     def submit(self, reqs: np.ndarray, n: int | None = None):
         """End-to-end: H2D of the requests, execution, D2H of the status."""
         n = len(reqs) if n is None else n

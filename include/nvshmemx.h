@@ -93,6 +93,8 @@ long long nvshmemx_status_detail(void);
 void nvshmemx_set_error_mode(int mode);
 int nvshmemx_get_error_mode(void);
 const char *nvshmemx_strerror(int code);
+/* Message of the most recent host-side failure ("" if none yet). */
+const char *nvshmemx_last_error_string(void);
 
 /* ---- host: arena queries and direct access ------------------------------ */
 void *nvshmemx_arena_base(void);

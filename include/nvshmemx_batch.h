@@ -76,8 +76,13 @@ int nvshmemx_batch_execute(nvshmemx_batch *b, int reps, float *out_ms);
 int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n, int *out_status,
                           float *out_ms);
 
-/* Statistics of the last execution: chunk count and the kernel time of the
- * exec kernel alone (CUDA events around it inside the last execution). */
+/* The same work as nvshmemx_batch_execute, enqueued without a graph and with
+ * CUDA events around the plan and exec kernels on the batch's stream:
+ * *out_ms is the time of all reps, *out_exec_ms the exec kernel's share. */
+int nvshmemx_batch_execute_direct(nvshmemx_batch *b, int reps, float *out_ms, float *out_exec_ms);
+
+/* Statistics of the last execution: chunk count, and the plan and exec kernel
+ * times of the last nvshmemx_batch_execute_direct (0 before one ran). */
 int nvshmemx_batch_last_stats(const nvshmemx_batch *b, unsigned long long *chunks, float *plan_ms,
                               float *exec_ms);
 

@@ -41,6 +41,8 @@ def test_c4_small_bit_exact(shmem_factory, cfg):
         b.upload(reqs)
         b.execute(1)
         b.execute(2)  # idempotent: sources never overlap destinations
+        total, exec_ms = b.execute_direct(1)
+        assert 0 < exec_ms <= total
         chunks, _, _ = b.stats()
         assert chunks >= len(reqs) - np.count_nonzero(reqs["bytes"] == 0) // 2
     assert sh.status() == 0

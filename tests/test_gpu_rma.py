@@ -49,17 +49,18 @@ def test_random_requests_bit_exact(shmem_factory, mode):
 def test_put_get_lengths(shmem_factory, dtype, nelems):
     """Every length, including 0 and lengths that leave ragged heads/tails."""
     w = 8 if dtype == DT_DOUBLE else 4
-    sh, om = start(shmem_factory, 2)
-    rows = [dict(src_off=64 + 4, dst_off=HEAP // 2 + 8, bytes=nelems * w, src_pe=0, dst_pe=1,
+    heap = 4 << 20
+    sh, om = start(shmem_factory, 2, heap=heap)
+    rows = [dict(src_off=64 + 4, dst_off=heap // 2 + 8, bytes=nelems * w, src_pe=0, dst_pe=1,
                  op=REQ_PUT, dtype=dtype),
-            dict(src_off=128, dst_off=HEAP // 2 + 200000 + 4 * (w == 4), bytes=nelems * w, src_pe=1,
+            dict(src_off=128, dst_off=3 * heap // 4 + 4 * (w == 4), bytes=nelems * w, src_pe=1,
                  dst_pe=0, op=REQ_GET, dtype=dtype)]
     reqs = requests(rows)
     for mode in MODES:
         sh.exec_requests(reqs, mode)
         assert sh.status() == 0
     om.apply_requests(reqs)
-    assert first_diff(heap_images(sh, 2, HEAP), om.heap) is None
+    assert first_diff(heap_images(sh, 2, heap), om.heap) is None
 
 
 def test_p_g_all_types(shmem_factory):
