@@ -31,6 +31,8 @@ sys.path.insert(0, ROOT)
 METRIC = "batched put/get GB/s (% HBM peak) vs per-call path; p50 wait/barrier ns; 1 B200"
 UNIT = "GB/s"
 C4 = dict(seed=4, n=100_000, npes=64, heap=64 << 20)
+# a quarter-size case of the same kernel for ncu captures (1 GiB arena)
+C4_SMALL = dict(seed=4, n=25_000, npes=16, heap=64 << 20)
 WORKLOAD = ("C4 batched uneven traffic: 64 virtual PEs x 64 MiB heap, 100,000 put/get/signal "
             "requests per batch, log-normal sizes median 2 KiB sigma 1.5 clipped 4 B..4 MiB, "
             "put 45%/get 45%/signal 10%, uniform PE pairs, disjoint 16-B-aligned destinations, seed 4")
@@ -180,6 +182,47 @@ def load_tuned():
     return None
 
 
+def run_extras(peak):
+    """Latency metrics (C1 ping-pong, device barrier on 8 PEs) and C2 bulk
+    all-to-all throughput (8 PEs, rotating buffer sets larger than 2x L2)."""
+    import numpy as np
+    from nvshmem_b200 import MODE_BLOCK, MODE_BULK, REQ_PUT, DT_FLOAT, Shmem
+    out = {}
+    with Shmem(2, 8 << 20) as sh:
+        flag = sh.alloc(4)
+        ns, _ = sh.pingpong(flag, 0, 0, 10000, 20)
+        out["pingpong_rtt_ns"] = {"p50": round(float(np.percentile(ns, 50)), 1),
+                                  "p99": round(float(np.percentile(ns, 99)), 1), "iters": 10000}
+    with Shmem(8, 1 << 20) as sh:
+        bar = {}
+        for ctas in (1, 16):
+            ns, _ = sh.barrier_latency(ctas, 10000)
+            bar[f"{ctas}_cta_per_pe"] = {"p50": round(float(np.percentile(ns, 50)), 1),
+                                         "p99": round(float(np.percentile(ns, 99)), 1)}
+        out["barrier_ns"] = bar
+        out["offload_barrier_us_per_call"] = round(sh.offload_barrier(1000), 3)
+    # C2 bulk all-to-all: 8 PEs, 1 MiB and 16 MiB messages, rotating sets > 2x L2
+    a2a = {}
+    for nbytes in (1 << 20, 16 << 20):
+        nsets = max(2, (512 << 20) // (2 * 8 * 8 * nbytes) + 1)
+        heap = 2 * 8 * nbytes * nsets
+        with Shmem(8, heap) as sh:
+            for pe in range(8):
+                sh.fill_random(pe, 0, heap, 1)
+            rounds = 4 * nsets
+            for mode, name in ((MODE_BLOCK, "block"), (MODE_BULK, "bulk")):
+                ctas = 18 if name == "block" else 18
+                sh.alltoall(REQ_PUT, DT_FLOAT, 0, 8 * nbytes, nbytes, rounds=nsets, nsets=nsets,
+                            set_stride=16 * nbytes, mode=mode, ctas_per_pe=ctas)
+                ms = sh.alltoall(REQ_PUT, DT_FLOAT, 0, 8 * nbytes, nbytes, rounds=rounds, nsets=nsets,
+                                 set_stride=16 * nbytes, mode=mode, ctas_per_pe=ctas)
+                gbs = 2 * 8 * 7 * nbytes * rounds / (ms / 1e3) / 1e9
+                a2a[f"{nbytes >> 20}MiB_{name}"] = {"GBps": round(gbs, 1), "frac": round(gbs / peak, 3)}
+            assert sh.status() == 0
+    out["alltoall_8pe"] = a2a
+    return out
+
+
 def run_gpu(args, rank, world, local):
     import numpy as np
     import torch
@@ -191,6 +234,7 @@ def run_gpu(args, rank, world, local):
     dist = dist_init(world)
     peak, peak_kind = measured_peak()
     flush = l2_flusher()
+    C4 = globals()["C4"] if args.workload == "c4" else C4_SMALL
     reqs = c4_batch(**C4)
     alg = requests_bytes(reqs)
     payload = int(reqs["bytes"].sum())
@@ -252,39 +296,8 @@ def run_gpu(args, rank, world, local):
                 cfg_used = b.config()
             assert sh.status() == 0
             checks = [sh.checksum(pe, 0, C4["heap"]) for pe in range(C4["npes"])]
-        # latency metrics: ping-pong (C1) and device barrier (8 PEs)
-        with Shmem(2, 8 << 20) as sh:
-            flag = sh.alloc(4)
-            ns, _ = sh.pingpong(flag, 0, 0, 10000, 20)
-            out["pingpong_rtt_ns"] = {"p50": round(float(np.percentile(ns, 50)), 1),
-                                      "p99": round(float(np.percentile(ns, 99)), 1), "iters": 10000}
-        with Shmem(8, 1 << 20) as sh:
-            bar = {}
-            for ctas in (1, 16):
-                ns, _ = sh.barrier_latency(ctas, 10000)
-                bar[f"{ctas}_cta_per_pe"] = {"p50": round(float(np.percentile(ns, 50)), 1),
-                                             "p99": round(float(np.percentile(ns, 99)), 1)}
-            out["barrier_ns"] = bar
-            out["offload_barrier_us_per_call"] = round(sh.offload_barrier(1000), 3)
-        # C2 bulk all-to-all: 8 PEs, 1 MiB and 16 MiB messages, rotating sets > 2x L2
-        a2a = {}
-        for nbytes in (1 << 20, 16 << 20):
-            nsets = max(2, (512 << 20) // (2 * 8 * 8 * nbytes) + 1)
-            heap = 2 * 8 * nbytes * nsets
-            with Shmem(8, heap) as sh:
-                for pe in range(8):
-                    sh.fill_random(pe, 0, heap, 1)
-                rounds = 4 * nsets
-                for mode, name in ((MODE_BLOCK, "block"), (MODE_BULK, "bulk")):
-                    ctas = 18 if name == "block" else 18
-                    sh.alltoall(REQ_PUT, DT_FLOAT, 0, 8 * nbytes, nbytes, rounds=nsets, nsets=nsets,
-                                set_stride=16 * nbytes, mode=mode, ctas_per_pe=ctas)
-                    ms = sh.alltoall(REQ_PUT, DT_FLOAT, 0, 8 * nbytes, nbytes, rounds=rounds, nsets=nsets,
-                                     set_stride=16 * nbytes, mode=mode, ctas_per_pe=ctas)
-                    gbs = 2 * 8 * 7 * nbytes * rounds / (ms / 1e3) / 1e9
-                    a2a[f"{nbytes >> 20}MiB_{name}"] = {"GBps": round(gbs, 1), "frac": round(gbs / peak, 3)}
-                assert sh.status() == 0
-        out["alltoall_8pe"] = a2a
+        if args.only != "batch":
+            out.update(run_extras(peak))
     clocks = sampler.summary()
 
     value = world * alg * args.steps / t_batch / 1e9
@@ -331,6 +344,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="c4", choices=["c4", "c4-small"])
+    ap.add_argument("--only", default="all", choices=["all", "batch"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
