@@ -16,6 +16,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <mutex>
+
 #include "batch.h"
 #include "nvshmemx_batch.h"
 
@@ -506,3 +508,104 @@ int nvshmemx_batch_execute_percall(nvshmemx_batch *b, int mode, int reps, float 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free batch execution (nvshmemx_batch_execute_noalloc).
+//
+// A batch normally gets its scratch -- the 32-byte control block and the
+// table of 32-byte work items the plan kernel fills -- from cudaMalloc in
+// nvshmemx_batch_create.  Some callers cannot do that: a serving loop that
+// must not take the device-wide synchronisation and unbounded latency of
+// cudaMalloc between requests, a process whose device memory belongs to
+// another allocator (a framework's caching pool, or a budget fixed at start-up
+// that leaves nothing to allocate later), or a foreign-language caller that
+// has no way to release device memory it would have to own.  For them the
+// scratch below is a file-scope device array that every GPU loading this
+// library holds until the process exits.
+//
+// Host code must not pass g_noalloc_scratch itself to a kernel: on the host
+// that name is only a stand-in, not a device address.  The device address is
+// looked up once per device with cudaGetSymbolAddress, with that device
+// current, on the first call made on it.
+namespace nvshm {
+
+static const unsigned long long kNoallocMaxItems = NVSHMEMX_NOALLOC_MAX_CHUNKS;
+static const size_t kNoallocCtlBytes = 256;  // BatchCtl, padded to keep the table aligned
+
+static __device__ __align__(256) unsigned char
+    g_noalloc_scratch[kNoallocCtlBytes + NVSHMEMX_NOALLOC_MAX_CHUNKS * sizeof(WorkItem)];
+
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_addr[128];  // device address of g_noalloc_scratch per device ordinal
+
+static int noalloc_scratch(void **out) {
+  int dev = 0;
+  int rc;
+  if ((rc = check_cuda(cudaGetDevice(&dev), "cudaGetDevice"))) return rc;
+  if (dev < 0 || dev >= 128) return fail(NVSHMEMX_ERR_UNSUPPORTED, "batch_execute_noalloc: device ordinal %d", dev);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    if ((rc = check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(noalloc scratch)")))
+      return rc;
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return 0;
+}
+
+}  // namespace nvshm
+
+extern "C" int nvshmemx_batch_execute_noalloc(const nvshmemx_request *d_reqs, int n, const nvshmemx_batch_config *cfg,
+                                              void *stream) {
+  if (!is_started()) return fail(NVSHMEMX_ERR_STATE, "batch_execute_noalloc before nvstart_pes");
+  if (n < 0 || (n > 0 && !d_reqs)) return fail(NVSHMEMX_ERR_INVALID, "batch_execute_noalloc: bad request array");
+  if ((unsigned long long)n > kNoallocMaxItems)
+    return fail(NVSHMEMX_ERR_NOMEM,
+                "batch_execute_noalloc: %d requests exceed the fixed scratch of %llu work items; use "
+                "nvshmemx_batch_create for larger batches",
+                n, kNoallocMaxItems);
+  nvshmemx_batch_config k;
+  if (cfg) {
+    if (check_batch_config(*cfg)) return fail(NVSHMEMX_ERR_INVALID, "batch_execute_noalloc: invalid configuration");
+    k = *cfg;
+  } else {
+    nvshmemx_batch_default_config(&k);
+  }
+  ExecFn fn = pick_exec(k.vec_bytes, k.unroll);
+  if (!fn) return fail(NVSHMEMX_ERR_INVALID, "batch_execute_noalloc: no kernel for this configuration");
+  void *scratch = nullptr;
+  int rc;
+  if ((rc = noalloc_scratch(&scratch))) return rc;
+  BatchCtl *ctl = reinterpret_cast<BatchCtl *>(scratch);
+  WorkItem *items = reinterpret_cast<WorkItem *>(static_cast<char *>(scratch) + kNoallocCtlBytes);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const Runtime &r = rt();
+  (void)cudaGetLastError();
+  // The array keeps the previous call's contents: the control block (chunk
+  // count, cursor, status) must start at zero; the work-item table is fully
+  // rewritten by the plan kernel before the exec kernel reads it.
+  if ((rc = check_cuda(cudaMemsetAsync(ctl, 0, sizeof(BatchCtl), s), "cudaMemsetAsync(noalloc control)"))) return rc;
+  if (n > 0)
+    batch_plan_kernel<<<(n + 255) / 256, 256, 0, s>>>(r.cfg, d_reqs, n, (unsigned)k.chunk_bytes, items,
+                                                      kNoallocMaxItems, ctl);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, k.threads, 0);
+  if (per_sm < 1) per_sm = 1;
+  const int ctas = k.ctas_per_sm > 0 && k.ctas_per_sm < per_sm ? k.ctas_per_sm : per_sm;
+  fn<<<r.sm_count * ctas, k.threads, 0, s>>>(items, ctl, kNoallocMaxItems, k.grab);
+  if ((rc = check_cuda(cudaGetLastError(), "batch_execute_noalloc launch"))) return rc;
+  int st[2] = {0, 0};
+  if ((rc = check_cuda(cudaMemcpyAsync(st, &ctl->status, sizeof st, cudaMemcpyDeviceToHost, s),
+                       "cudaMemcpyAsync(noalloc status)")))
+    return rc;
+  if ((rc = check_cuda(cudaStreamSynchronize(s), "batch_execute_noalloc"))) return rc;
+  if (st[0] == NVSHMEMX_ERR_NOMEM)
+    return fail(NVSHMEMX_ERR_NOMEM,
+                "batch_execute_noalloc: the batch needs more than %llu chunks of %d bytes; nothing was executed",
+                kNoallocMaxItems, k.chunk_bytes);
+  if (st[0])
+    return fail(st[0], "batch_execute_noalloc: request %d rejected (%s); nothing was executed", st[1],
+                nvshmemx_strerror(st[0]));
+  return 0;
+}

@@ -124,6 +124,7 @@ _SIGS = {
     "nvshmemx_batch_last_stats": (c_int, [c_void_p, _P(c_ulonglong), _P(c_float), _P(c_float)]),
     "nvshmemx_requests_bytes": (c_ulonglong, [c_void_p, c_int]),
     "nvshmemx_batch_execute_percall": (c_int, [c_void_p, c_int, c_int, _P(c_float)]),
+    "nvshmemx_batch_execute_noalloc": (c_int, [c_void_p, c_int, _P(BatchConfig), c_void_p]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

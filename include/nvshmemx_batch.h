@@ -95,6 +95,41 @@ unsigned long long nvshmemx_requests_bytes(const nvshmemx_request *reqs, int n);
  * launches back to back; *out_ms the device time of all reps. */
 int nvshmemx_batch_execute_percall(nvshmemx_batch *b, int mode, int reps, float *out_ms);
 
+/* Work items (chunks) the allocation-free entry point below can hold:
+ * 32768 x 32 bytes = 1 MiB of scratch, plus a 256-byte control block. */
+#define NVSHMEMX_NOALLOC_MAX_CHUNKS 32768
+
+/* Allocation-free batch execution.  No counterpart in the reference (the
+ * prototype has no batching at all).
+ *
+ * Executes n requests that are already in device memory (d_reqs, owned by
+ * the caller) on `stream` (a cudaStream_t; NULL for the legacy default
+ * stream) and waits for them, without allocating: it calls no cudaMalloc,
+ * cudaFree or allocating library routine.  It is for callers that cannot
+ * allocate device memory while they run -- a serving loop that must not take
+ * cudaMalloc's device-wide synchronisation and unbounded latency, a process
+ * whose device memory is owned by another allocator or a budget fixed at
+ * start-up, a foreign-language caller that cannot release device memory it
+ * would have to own.
+ *
+ * Its scratch is a fixed array inside this library that every GPU loading
+ * the library holds until the process exits.  Limits: at most
+ * NVSHMEMX_NOALLOC_MAX_CHUNKS requests and at most that many chunks of
+ * cfg->chunk_bytes in total; larger batches are rejected with
+ * NVSHMEMX_ERR_NOMEM and nothing is executed.  cfg NULL uses
+ * nvshmemx_batch_default_config.
+ *
+ * The first call on a device looks up the scratch array's device address
+ * (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture.  All calls share the one array: the control
+ * block is cleared at the start of every call, so sequential calls are
+ * independent, but calls whose executions overlap on the GPU (from several
+ * host threads or streams at once) race on it and must be serialised by the
+ * caller.  Results are bit-identical to nvshmemx_batch_execute on the same
+ * requests. */
+int nvshmemx_batch_execute_noalloc(const nvshmemx_request *d_reqs, int n, const nvshmemx_batch_config *cfg,
+                                   void *stream);
+
 #ifdef __cplusplus
 }
 #endif
