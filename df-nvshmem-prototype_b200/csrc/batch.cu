@@ -156,9 +156,11 @@ __device__ __forceinline__ void run_item(const WorkItem &w, unsigned lane) {
   if (w.kind == kCopy) {
     copy_coop<VB, U>(reinterpret_cast<char *>(w.dst), reinterpret_cast<const char *>(w.src), w.len, lane, 32);
   } else if (lane == 0) {
+    // Requests of one batch are unordered with respect to each other (they
+    // touch disjoint bytes), so a SIGNAL is a plain 4-byte store like
+    // nvshmem_int_p; completion of the batch orders it before later work.
     if (w.kind == kSignal) {
-      fence_gpu();
-      st_release_b32(reinterpret_cast<void *>(w.dst), (unsigned)w.value);
+      st_relaxed_b32(reinterpret_cast<void *>(w.dst), (unsigned)w.value);
     } else if (w.len == 8) {
       st_relaxed_b64(reinterpret_cast<void *>(w.dst), w.src);
     } else {

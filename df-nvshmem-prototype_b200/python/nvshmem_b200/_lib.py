@@ -51,6 +51,11 @@ class BatchConfig(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class TuneResult(ctypes.Structure):
+    _fields_ = [("cfg", BatchConfig), ("ms_median", c_float), ("ms_min", c_float),
+                ("exec_ms_median", c_float), ("status", c_int)]
+
+
 class ShmemError(RuntimeError):
     def __init__(self, code: int, what: str):
         self.code = code
@@ -125,6 +130,10 @@ _SIGS = {
     "nvshmemx_requests_bytes": (c_ulonglong, [c_void_p, c_int]),
     "nvshmemx_batch_execute_percall": (c_int, [c_void_p, c_int, c_int, _P(c_float)]),
     "nvshmemx_batch_execute_noalloc": (c_int, [c_void_p, c_int, _P(BatchConfig), c_void_p]),
+    # nvshmemx_tune.h
+    "nvshmemx_tune_candidates": (c_int, [_P(BatchConfig), c_int, c_int]),
+    "nvshmemx_tune_batch": (c_int, [c_void_p, _P(BatchConfig), c_int, c_int, c_size_t, _P(TuneResult),
+                                    _P(c_int)]),
 }
 
 for _name, (_res, _args) in _SIGS.items():
