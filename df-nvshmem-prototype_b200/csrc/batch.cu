@@ -194,6 +194,133 @@ __global__ void __launch_bounds__(1024) batch_exec_kernel(const WorkItem *__rest
   }
 }
 
+// ------------------------------------------------------- exec through TMA
+// Same claiming loop as batch_exec_kernel, but the 16-byte-aligned body of
+// every copy chunk goes through a per-warp ring of S shared-memory stages:
+// lane 0 issues cp.async.bulk global->shared (completion counted on the
+// stage's mbarrier) and, once a stage has landed, cp.async.bulk
+// shared->global as one bulk group.  The ring spans work items, so each warp
+// keeps up to S loads in flight across chunk boundaries without holding the
+// data in registers; lanes 1..31 copy the unaligned head and tail bytes.
+// Chunks whose source and destination differ in alignment modulo 16, or that
+// are shorter than min_bulk, take the register copy.
+struct WarpRing {
+  unsigned long long *mbar;  // S mbarriers
+  unsigned long long *pdst;  // destination of the piece in each stage
+  unsigned *plen;            // length of the piece in each stage
+  char *buf;                 // S * SB bytes
+};
+
+__device__ __forceinline__ void bulk_wait_read_le(unsigned n) {
+  switch (n) {
+    case 0: asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); break;
+    case 1: asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); break;
+    case 2: asm volatile("cp.async.bulk.wait_group.read 2;" ::: "memory"); break;
+    default: asm volatile("cp.async.bulk.wait_group.read 3;" ::: "memory"); break;
+  }
+}
+
+template <int S>
+__global__ void __launch_bounds__(256) batch_exec_tma_kernel(const WorkItem *__restrict__ items, BatchCtl *ctl,
+                                                              unsigned long long cap, int grab, unsigned SB,
+                                                              unsigned min_bulk, long long timeout_ns) {
+  extern __shared__ __align__(128) char smem[];
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  char *base = smem + (size_t)warp * (256 + (size_t)S * SB);
+  WarpRing ring;
+  ring.mbar = reinterpret_cast<unsigned long long *>(base);
+  ring.pdst = reinterpret_cast<unsigned long long *>(base + 64);
+  ring.plen = reinterpret_cast<unsigned *>(base + 128);
+  ring.buf = base + 256;
+  if (*(volatile int *)&ctl->status != 0) return;
+  const unsigned long long C = *(volatile unsigned long long *)&ctl->total_chunks;
+  if (C > cap) return;
+  unsigned issued = 0, retired = 0;
+  bool ok = true;
+  const unsigned long long deadline = gtimer() + (unsigned long long)timeout_ns;
+  if (lane == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(ring.mbar + s, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncwarp();
+  // lane 0: wait for the oldest piece to land, then store it from its stage
+  auto retire_one = [&]() {
+    const unsigned p = retired, s = p % S;
+    if (ok && !mbar_wait(ring.mbar + s, (p / S) & 1u, deadline)) ok = false;
+    if (ok) {
+      bulk_s2g(reinterpret_cast<void *>(ring.pdst[s]), ring.buf + (size_t)s * SB, ring.plen[s]);
+      bulk_commit();
+    }
+    ++retired;
+  };
+  unsigned long long bse = 0;
+  if (lane == 0) bse = atomicAdd(&ctl->cursor, (unsigned long long)grab);
+  bse = __shfl_sync(0xffffffffu, bse, 0);
+  while (bse < C) {
+    unsigned long long nxt = 0;
+    if (lane == 0) nxt = atomicAdd(&ctl->cursor, (unsigned long long)grab);
+    const unsigned long long end = bse + grab < C ? bse + grab : C;
+    for (unsigned long long k = bse; k < end; ++k) {
+      const WorkItem w = load_item(items + k);
+      char *d = reinterpret_cast<char *>(w.dst);
+      const char *s = reinterpret_cast<const char *>(w.src);
+      if (w.kind != kCopy || (((uintptr_t)d ^ (uintptr_t)s) & 15) != 0 || w.len < min_bulk) {
+        run_item<16, 4>(w, lane);
+        continue;
+      }
+      unsigned head = (unsigned)((16 - ((uintptr_t)d & 15)) & 15);
+      if (head > w.len) head = w.len;
+      const unsigned body = (w.len - head) & ~15u;
+      const unsigned tail = w.len - head - body;
+      if (lane != 0) {
+        for (unsigned i = lane - 1; i < head; i += 31) d[i] = s[i];
+        for (unsigned i = lane - 1; i < tail; i += 31) d[head + body + i] = s[head + body + i];
+      } else if (ok) {
+        for (unsigned off = 0; off < body && ok; off += SB) {
+          const unsigned len = body - off < SB ? body - off : SB;
+          if (issued - retired == (unsigned)S) retire_one();
+          const unsigned st = issued % S;
+          // the store that last read this stage (piece issued - S) must be
+          // done reading: at most `after` younger stores may still be pending
+          if (issued >= (unsigned)S) bulk_wait_read_le(retired - 1u - (issued - (unsigned)S));
+          ring.pdst[st] = (unsigned long long)(d + head + off);
+          ring.plen[st] = len;
+          mbar_expect_tx(ring.mbar + st, len);
+          bulk_g2s(ring.buf + (size_t)st * SB, s + head + off, len, ring.mbar + st);
+          ++issued;
+        }
+      }
+      __syncwarp();
+    }
+    bse = __shfl_sync(0xffffffffu, nxt, 0);
+  }
+  if (lane == 0) {
+    while (retired < issued) retire_one();
+    bulk_wait_all();
+    if (!ok) {
+      if (atomicCAS(&ctl->status, 0, NVSHMEMX_ERR_TIMEOUT) == 0) ctl->bad_request = -2;
+    } else {
+      for (int s = 0; s < S; ++s) mbar_inval(ring.mbar + s);
+    }
+  }
+}
+
+typedef void (*TmaFn)(const WorkItem *, BatchCtl *, unsigned long long, int, unsigned, unsigned, long long);
+
+static TmaFn pick_tma(int stages) {
+  switch (stages) {
+    case 2: return batch_exec_tma_kernel<2>;
+    case 3: return batch_exec_tma_kernel<3>;
+    case 4: return batch_exec_tma_kernel<4>;
+    default: return nullptr;
+  }
+}
+
+static size_t tma_smem_bytes(const nvshmemx_batch_config &k) {
+  return (size_t)(k.threads / 32) * (256 + (size_t)k.tma_stages * (size_t)k.tma_stage_bytes);
+}
+
 typedef void (*ExecFn)(const WorkItem *, BatchCtl *, unsigned long long, int);
 
 static ExecFn pick_exec(int vb, int u) {
@@ -212,7 +339,15 @@ int check_batch_config(const nvshmemx_batch_config &c) {
                   (c.unroll == 1 || c.unroll == 2 || c.unroll == 4 || c.unroll == 8) &&
                   (c.threads == 128 || c.threads == 256 || c.threads == 512 || c.threads == 1024) &&
                   c.ctas_per_sm >= 0 && c.ctas_per_sm <= 16 && c.grab >= 1 && c.grab <= 16;
-  return ok ? 0 : NVSHMEMX_ERR_INVALID;
+  if (!ok) return NVSHMEMX_ERR_INVALID;
+  if (c.tma_stages == 0) return 0;
+  // TMA rings: at most 256 threads per CTA (8 warps, one ring each), stage
+  // sizes in whole KiB, and the CTA's rings must fit in 227 KiB of shared
+  // memory.
+  const bool tma_ok = (c.tma_stages >= 2 && c.tma_stages <= 4) && c.threads <= 256 && c.tma_stage_bytes >= 1024 &&
+                      c.tma_stage_bytes <= 32768 && (c.tma_stage_bytes % 1024) == 0 && c.tma_min_bytes >= 0 &&
+                      tma_smem_bytes(c) <= 227u * 1024u;
+  return tma_ok ? 0 : NVSHMEMX_ERR_INVALID;
 }
 
 }  // namespace nvshm
@@ -255,10 +390,19 @@ static int enqueue_batch(nvshmemx_batch *b, bool with_events) {
   const Cfg c = r.cfg;
   const nvshmemx_batch_config &k = b->cfg;
   ExecFn fn = pick_exec(k.vec_bytes, k.unroll);
-  if (!fn) return fail(NVSHMEMX_ERR_INVALID, "batch: no kernel for vec %d unroll %d", k.vec_bytes, k.unroll);
+  TmaFn tfn = k.tma_stages ? pick_tma(k.tma_stages) : nullptr;
+  if (!fn || (k.tma_stages && !tfn))
+    return fail(NVSHMEMX_ERR_INVALID, "batch: no kernel for vec %d unroll %d stages %d", k.vec_bytes, k.unroll,
+                k.tma_stages);
   (void)cudaGetLastError();  // report only this enqueue's own launch errors
+  const size_t smem = tfn ? tma_smem_bytes(k) : 0;
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, k.threads, 0);
+  if (tfn) {
+    cudaFuncSetAttribute((const void *)tfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)tfn, k.threads, smem);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, k.threads, 0);
+  }
   if (per_sm < 1) per_sm = 1;
   int ctas = k.ctas_per_sm > 0 && k.ctas_per_sm < per_sm ? k.ctas_per_sm : per_sm;
   cudaMemsetAsync(b->d_ctl, 0, sizeof(BatchCtl), b->stream);
@@ -267,7 +411,12 @@ static int enqueue_batch(nvshmemx_batch *b, bool with_events) {
     batch_plan_kernel<<<(b->n + 255) / 256, 256, 0, b->stream>>>(c, b->d_reqs, b->n, (unsigned)k.chunk_bytes,
                                                                  b->d_items, b->cap, b->d_ctl);
   if (with_events) cudaEventRecord(b->ev_exec0, b->stream);
-  fn<<<r.sm_count * ctas, k.threads, 0, b->stream>>>(b->d_items, b->d_ctl, b->cap, k.grab);
+  if (tfn)
+    tfn<<<r.sm_count * ctas, k.threads, smem, b->stream>>>(b->d_items, b->d_ctl, b->cap, k.grab,
+                                                             (unsigned)k.tma_stage_bytes, (unsigned)k.tma_min_bytes,
+                                                             c.wait_timeout_ns);
+  else
+    fn<<<r.sm_count * ctas, k.threads, 0, b->stream>>>(b->d_items, b->d_ctl, b->cap, k.grab);
   if (with_events) cudaEventRecord(b->ev_exec1, b->stream);
   return check_cuda(cudaGetLastError(), "batch launch");
 }
@@ -309,6 +458,9 @@ void nvshmemx_batch_default_config(nvshmemx_batch_config *c) {
   c->threads = 512;
   c->ctas_per_sm = 2;
   c->grab = 2;
+  c->tma_stages = 0;
+  c->tma_stage_bytes = 8192;
+  c->tma_min_bytes = 1024;
 }
 
 int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes, int min_chunk_bytes,

@@ -47,27 +47,42 @@ using namespace nvshm;
 extern "C" {
 
 int nvshmemx_tune_candidates(nvshmemx_batch_config *out, int max, int min_chunk_bytes) {
-  static const int vecs[] = {16, 8};
-  static const int unrolls[] = {2, 4, 8};
-  static const int chunks[] = {4096, 16384, 65536};
-  static const int threads[] = {256, 512, 1024};
-  static const int grabs[] = {1, 2, 4};
   int n = 0;
-  for (int v : vecs)
-    for (int u : unrolls)
-      for (int ch : chunks)
-        for (int t : threads)
-          for (int g : grabs) {
-            if (ch < min_chunk_bytes) continue;
-            if (n >= max) return n;
-            nvshmemx_batch_config c;
-            c.vec_bytes = v;
-            c.unroll = u;
+  auto push = [&](const nvshmemx_batch_config &c) {
+    if (n < max && c.chunk_bytes >= min_chunk_bytes && check_batch_config(c) == 0) out[n++] = c;
+  };
+  nvshmemx_batch_config c;
+  nvshmemx_batch_default_config(&c);
+  // copies through registers: accesses in flight x chunk x threads x claim
+  for (int u : {2, 4, 8})
+    for (int ch : {4096, 16384, 65536})
+      for (int t : {256, 1024})
+        for (int g : {1, 2, 4}) {
+          c.vec_bytes = 16;
+          c.unroll = u;
+          c.chunk_bytes = ch;
+          c.threads = t;
+          c.ctas_per_sm = 0;
+          c.grab = g;
+          c.tma_stages = 0;
+          push(c);
+        }
+  // TMA rings: stages x stage size x warps per CTA x chunk x bulk threshold
+  for (int s : {2, 3, 4})
+    for (int sb : {4096, 8192, 16384})
+      for (int t : {128, 256})
+        for (int ch : {16384, 65536})
+          for (int mb : {512, 2048}) {
+            c.vec_bytes = 16;
+            c.unroll = 4;
             c.chunk_bytes = ch;
             c.threads = t;
             c.ctas_per_sm = 0;
-            c.grab = g;
-            out[n++] = c;
+            c.grab = 2;
+            c.tma_stages = s;
+            c.tma_stage_bytes = sb;
+            c.tma_min_bytes = mb;
+            push(c);
           }
   return n;
 }

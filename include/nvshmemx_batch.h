@@ -37,13 +37,18 @@ typedef struct nvshmemx_batch_config {
   int vec_bytes;    /* widest access: 4, 8 or 16                              */
   int chunk_bytes;  /* work unit: multiple of 256 in [256, 1 MiB]             */
   int unroll;       /* accesses in flight per lane: 1, 2, 4 or 8              */
-  int threads;      /* threads per CTA: 128, 256, 512 or 1024                 */
+  int threads;      /* threads per CTA: 128, 256, 512 or 1024 (TMA: <= 256)   */
   int ctas_per_sm;  /* resident CTAs per SM (0: as many as fit)               */
   int grab;         /* chunks claimed per cursor atomic: 1..16                */
+  int tma_stages;   /* 0: copy through registers; 2, 3 or 4: every warp
+                       streams 16-byte-aligned bodies through a ring of this
+                       many shared-memory stages with cp.async.bulk          */
+  int tma_stage_bytes; /* bytes per stage: multiple of 1024, 1 KiB..32 KiB    */
+  int tma_min_bytes;   /* chunks shorter than this use the register copy    */
 } nvshmemx_batch_config;
 
-/* Sensible defaults for B200 (16-byte vectors, 16 KiB chunks, 4 in flight,
- * 512 threads, 2 CTAs per SM, 2 chunks per claim). */
+/* Defaults for B200: the best configuration the autotuner measured on the
+ * 64-PE, 100,000-request workload (see tuned/batch_c4.json). */
 void nvshmemx_batch_default_config(nvshmemx_batch_config *cfg);
 
 typedef struct nvshmemx_batch nvshmemx_batch;

@@ -278,7 +278,10 @@ int main(int argc, char **argv) {
   else if (argc >= 5 && !strcmp(argv[1], "halo")) rc = scen_halo(atoi(argv[2]), atoi(argv[3]), argv[4]);
   else if (argc >= 5 && !strcmp(argv[1], "pingpong")) rc = scen_pingpong(atoi(argv[2]), atoi(argv[3]), strtoull(argv[4], 0, 10));
   nvshmem_barrier_all();
-  nvshmcleanup();
+  // The reference's nvshmcleanup frees its region list but leaves the list
+  // head and tail pointing at the freed entries (nvshmem.cu:805-819), so a
+  // second call double-frees; the alloc scenario has already called it.
+  if (!(argc >= 2 && !strcmp(argv[1], "alloc"))) nvshmcleanup();
   nvstop_pes();
   MPI_Finalize();
   return rc;

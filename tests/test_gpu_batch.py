@@ -18,6 +18,13 @@ CONFIGS = [
     dict(vec_bytes=16, chunk_bytes=256, unroll=1, threads=128, ctas_per_sm=1, grab=1),
     dict(vec_bytes=8, chunk_bytes=4096, unroll=8, threads=1024, ctas_per_sm=0, grab=16),
     dict(vec_bytes=4, chunk_bytes=65536, unroll=2, threads=256, ctas_per_sm=4, grab=4),
+    # TMA rings: every aligned chunk streamed through shared memory
+    dict(vec_bytes=16, chunk_bytes=16384, unroll=4, threads=256, ctas_per_sm=0, grab=2,
+         tma_stages=3, tma_stage_bytes=8192, tma_min_bytes=0),
+    dict(vec_bytes=16, chunk_bytes=65536, unroll=4, threads=128, ctas_per_sm=0, grab=4,
+         tma_stages=4, tma_stage_bytes=4096, tma_min_bytes=2048),
+    dict(vec_bytes=16, chunk_bytes=1024, unroll=4, threads=256, ctas_per_sm=1, grab=1,
+         tma_stages=2, tma_stage_bytes=1024, tma_min_bytes=16),
 ]
 
 
@@ -50,12 +57,14 @@ def test_c4_small_bit_exact(shmem_factory, cfg):
     assert first_diff(heap_images(sh, npes, heap), om.heap) is None
 
 
-def test_mixed_ops_and_alignments(shmem_factory):
+@pytest.mark.parametrize("tma", [0, 3])
+def test_mixed_ops_and_alignments(shmem_factory, tma):
     npes, heap = 8, 2 << 20
     reqs = random_requests(77, 800, npes, heap, max_bytes=40000)
     sh, om = setup(shmem_factory, npes, heap)
     with sh.batch(len(reqs), int(reqs["bytes"].sum()) + 8 * len(reqs), 256) as b:
-        b.set_config(dict(vec_bytes=16, chunk_bytes=1024, unroll=4, threads=256, ctas_per_sm=2, grab=2))
+        b.set_config(dict(vec_bytes=16, chunk_bytes=1024, unroll=4, threads=256, ctas_per_sm=2, grab=2,
+                          tma_stages=tma, tma_stage_bytes=2048, tma_min_bytes=0))
         b.upload(reqs)
         b.execute(1)
     assert sh.status() == 0
@@ -112,13 +121,17 @@ def test_empty_batch(shmem_factory):
     assert sh.status() == 0
 
 
-def test_c4_full_size_checksums(shmem_factory):
+@pytest.mark.parametrize("tma", [0, 3])
+def test_c4_full_size_checksums(shmem_factory, tma):
     """The benchmark's batch: 64 PEs x 64 MiB, 100,000 requests."""
     npes, heap = 64, 64 << 20
     reqs = c4_batch(seed=4, n=100_000, npes=npes, heap=heap)
     assert check_disjoint(reqs)
     sh, om = setup(shmem_factory, npes, heap, seed=44)
     with sh.batch(len(reqs), int(reqs["bytes"].sum()), 4096) as b:
+        if tma:
+            b.set_config(dict(vec_bytes=16, chunk_bytes=16384, unroll=4, threads=256, ctas_per_sm=0, grab=2,
+                              tma_stages=tma, tma_stage_bytes=8192, tma_min_bytes=1024))
         b.upload(reqs)
         b.execute(3)
     assert sh.status() == 0
