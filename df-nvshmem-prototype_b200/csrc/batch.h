@@ -16,4 +16,8 @@ int launch_exec_requests(int mode, const nvshmemx_request *d_reqs, int n, cudaSt
 // Validates a batch configuration; returns 0 or NVSHMEMX_ERR_INVALID.
 int check_batch_config(const nvshmemx_batch_config &c);
 
+// Writes `bytes` of a library-owned buffer and waits, so the next run does
+// not start with its data in L2 (tuner.cu).
+int l2_flush(size_t bytes);
+
 }  // namespace nvshm

@@ -131,6 +131,20 @@ _SIGS = {
     "nvshmemx_requests_bytes": (c_ulonglong, [c_void_p, c_int]),
     "nvshmemx_batch_execute_percall": (c_int, [c_void_p, c_int, c_int, _P(c_float)]),
     "nvshmemx_batch_execute_noalloc": (c_int, [c_void_p, c_int, _P(BatchConfig), c_void_p]),
+    # nvshmemx_picker.h
+    "nvshmemx_mlp_num_params": (c_int, []),
+    "nvshmemx_mlp_create": (c_int, [c_ulonglong, _P(c_void_p)]),
+    "nvshmemx_mlp_destroy": (c_int, [c_void_p]),
+    "nvshmemx_mlp_get_params": (c_int, [c_void_p, c_void_p]),
+    "nvshmemx_mlp_set_params": (c_int, [c_void_p, c_void_p]),
+    "nvshmemx_mlp_set_normalization": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "nvshmemx_mlp_forward": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
+    "nvshmemx_mlp_loss_grad": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, _P(c_float), c_void_p]),
+    "nvshmemx_mlp_train": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_float,
+                                   c_ulonglong, c_void_p]),
+    "nvshmemx_mlp_pick": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "nvshmemx_variant_time": (c_int, [c_void_p, c_int, c_int, c_size_t, _P(c_float)]),
+    "nvshmemx_variant_describe": (c_int, [c_int, _P(c_int), _P(BatchConfig)]),
     # nvshmemx_tune.h
     "nvshmemx_tune_candidates": (c_int, [_P(BatchConfig), c_int, c_int]),
     "nvshmemx_tune_batch": (c_int, [c_void_p, _P(BatchConfig), c_int, c_int, c_size_t, _P(TuneResult),

@@ -191,8 +191,11 @@ class Batch:
         self.close()
 
     def set_config(self, cfg: L.BatchConfig | dict):
+        """A BatchConfig, or a dict of fields over the defaults; a dict without
+        `tma_stages` selects the register copy."""
         if isinstance(cfg, dict):
             c = default_batch_config()
+            c.tma_stages = 0
             for k, v in cfg.items():
                 setattr(c, k, int(v))
             cfg = c

@@ -1,0 +1,317 @@
+"""Learned transfer-variant picker: data collection, training, picking and
+regret evaluation over the library's C ABI (include/nvshmemx_picker.h).
+
+A *request class* is a group of `inflight` requests of `size` bytes with one
+element width, relative alignment, PE count and traffic pattern:
+  pattern 0  PE pairs (the C1 ping-pong / put sweep shape)
+  pattern 1  all-to-all rounds (C2)
+  pattern 2  nearest-neighbour faces on a 3-D PE grid (C3)
+  pattern 3  uniform random PE pairs (C4)
+Every class is executed with each of the 12 variants (per-call thread, warp,
+CTA, CTA-TMA; batch-engine shapes with register or TMA copies), L2 flushed
+before every run; the median device time per variant is one training row.
+The network (own CUDA forward/backward/Adam kernels) learns log2 time per
+variant from the class features; the picker takes the fastest prediction and
+falls back to the measured table's nearest class when the features leave
+the training range.  Regret = total time of the picked variants over the
+exhaustive best, minus 1.
+
+  python -m nvshmem_b200.picker sweep [--out tuned/variant_timings.npz]
+  python -m nvshmem_b200.picker evaluate [--data tuned/variant_timings.npz]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import time
+from ctypes import byref, c_float, c_int, c_void_p
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import REQUEST_DTYPE, check, lib
+from .traffic import Stream
+
+NV = 12
+NI = 6
+VARIANT_NAMES = ["percall_thread", "percall_warp", "percall_cta", "percall_cta_tma",
+                 "batch_reg_4K_u4", "batch_reg_16K_u8", "batch_reg_64K_u4",
+                 "batch_tma_2x8K", "batch_tma_3x8K", "batch_tma_4x4K", "batch_tma_3x8K_64K",
+                 "batch_tma_2x16K_64K"]
+DEFAULT_VARIANT = 8  # the batch engine's default (autotuned) configuration
+ARENA_PES, ARENA_HEAP = 64, 64 << 20
+TUNED_DIR = os.path.join(L.PKG_ROOT, "tuned")
+DATA = os.path.join(TUNED_DIR, "variant_timings.npz")
+
+
+# ----------------------------------------------------------------- classes
+def features(size, width, align, npes, pattern, inflight):
+    return np.array([np.log2(size), width, np.log2(align), np.log2(npes), pattern, np.log2(inflight)],
+                    dtype=np.float32)
+
+
+def sample_classes(seed: int, n: int, patterns=(0, 1, 2)):
+    """n random classes; sizes 4 B..4 MiB, in-flight 1..4096, total <= 32 MiB."""
+    st = Stream(seed)
+    out = []
+    while len(out) < n:
+        lg = int(st.randint(1, 21)[0]) + 2                    # 2..22
+        width = 8 if st.uniform(1)[0] < 0.35 else 4
+        size = max(width, (1 << lg) // width * width)
+        align = [16, 8, 4][int(st.randint(1, 3)[0])]
+        if width == 8 and align == 4:
+            align = 8
+        npes = [2, 8, 64][int(st.randint(1, 3)[0])]
+        pattern = int(patterns[int(st.randint(1, len(patterns))[0])])
+        inflight = 1 << int(st.randint(1, 13)[0])             # 1..4096
+        per_pe_cap = (ARENA_HEAP // 2 - (1 << 20)) * min(npes, inflight)
+        while inflight > 1 and (inflight * (size + 32) > (32 << 20) or inflight * (size + 32) > per_pe_cap):
+            inflight //= 2
+        out.append(dict(size=size, width=width, align=align, npes=npes, pattern=pattern, inflight=inflight))
+    return out
+
+
+def _dst_pe(pattern, i, src, npes, st):
+    if pattern == 0:
+        return 1 - src if npes >= 2 else 0
+    if pattern == 1:
+        return (src + 1 + (i // npes) % max(npes - 1, 1)) % npes
+    if pattern == 2:
+        px = 2 if npes == 8 else (4 if npes == 64 else 2)
+        py = px if npes >= 8 else 1
+        x, y, z = src % px, (src // px) % py, src // (px * py)
+        pz = max(npes // (px * py), 1)
+        d = (i // npes) % 6
+        s = 1 if d & 1 else -1
+        if d < 2:
+            x = (x + s) % px
+        elif d < 4:
+            y = (y + s) % py
+        else:
+            z = (z + s) % pz
+        return (x + px * (y + py * z)) % npes
+    return int(st.randint(1, npes)[0])
+
+
+def make_group(c: dict, seed: int) -> np.ndarray:
+    """The requests of one class: alternating put/get, sources 16-byte aligned
+    in the lower half of the heap, destinations placed disjointly in the upper
+    half and offset by the class alignment modulo 16."""
+    st = Stream(seed)
+    n, npes, size = c["inflight"], c["npes"], c["size"]
+    skew = {16: 0, 8: 8, 4: 4}[c["align"]]
+    half = ARENA_HEAP // 2
+    r = np.zeros(n, dtype=REQUEST_DTYPE)
+    cursor = {}
+    for i in range(n):
+        src = i % npes if c["pattern"] in (1, 2) else (0 if c["pattern"] == 0 else int(st.randint(1, npes)[0]))
+        if c["pattern"] == 0 and i % 2:
+            src = 1 % npes
+        dst = _dst_pe(c["pattern"], i, src, npes, st)
+        slot = cursor.get(dst, half)
+        cursor[dst] = slot + (size + skew + 31) // 16 * 16
+        span = max((half - size - 64) // 16, 1)
+        r[i] = (int(st.randint(1, span)[0]) * 16, slot + skew, size, src, dst, i % 2,
+                2 if c["width"] == 8 else 1, 0, 0)
+    return r
+
+
+# ----------------------------------------------------------------- sweeps
+def measure(classes, seed0: int, reps: int = 3, flush_bytes: int = 256 << 20, log=None):
+    """Median device time (ms) of every variant on every class."""
+    from .api import Shmem
+    T = np.full((len(classes), NV), np.nan, dtype=np.float64)
+    with Shmem(ARENA_PES, ARENA_HEAP) as sh:
+        for pe in range(ARENA_PES):
+            sh.fill_random(pe, 0, ARENA_HEAP, 7)
+        with sh.batch(4096, 256 << 20, 1024) as b:
+            for ci, c in enumerate(classes):
+                g = make_group(c, seed0 + ci)
+                # halve the group until every destination fits its PE's heap
+                while c["inflight"] > 1 and int((g["dst_off"] + g["bytes"]).max()) > ARENA_HEAP:
+                    c["inflight"] //= 2
+                    g = make_group(c, seed0 + ci)
+                b.upload(g)
+                for v in range(NV):
+                    ms = c_float(0)
+                    rc = lib.nvshmemx_variant_time(b.h, v, reps, flush_bytes, byref(ms))
+                    if rc == 0:
+                        T[ci, v] = ms.value
+                    else:
+                        sh.status()
+                if log and ci % 50 == 0:
+                    log(f"class {ci}/{len(classes)} {c} best={VARIANT_NAMES[int(np.nanargmin(T[ci]))]}")
+        assert sh.status() == 0
+    return T
+
+
+def sweep(out: str = DATA, n_train: int = 600, n_mixes: int = 20, per_mix: int = 8, reps: int = 3, log=print):
+    t0 = time.time()
+    train = sample_classes(seed=2024, n=n_train, patterns=(0, 1, 2))  # C1..C3 traffic shapes
+    mixes = [sample_classes(seed=s, n=per_mix, patterns=(0, 1, 2, 3)) for s in range(100, 100 + n_mixes)]
+    held = [c for m in mixes for c in m]
+    Tt = measure(train, 10_000, reps, log=log)
+    Th = measure(held, 20_000, reps, log=log)
+    np.savez(out, train_x=np.stack([features(**c) for c in train]), train_t=Tt,
+             held_x=np.stack([features(**c) for c in held]), held_t=Th,
+             mix_of=np.repeat(np.arange(n_mixes), per_mix),
+             meta=json.dumps({"variants": VARIANT_NAMES, "reps": reps, "seconds": time.time() - t0,
+                              "train_seed": 2024, "mix_seeds": [100, 100 + n_mixes - 1]}))
+    return out
+
+
+# ----------------------------------------------------------------- network
+class MLP:
+    """The library's MLP (weights on the GPU)."""
+
+    def __init__(self, seed: int = 0):
+        self.h = c_void_p(0)
+        check(lib.nvshmemx_mlp_create(seed, byref(self.h)), "mlp_create")
+        self.nparam = lib.nvshmemx_mlp_num_params()
+
+    def close(self):
+        if self.h:
+            lib.nvshmemx_mlp_destroy(self.h)
+            self.h = c_void_p(0)
+
+    def __del__(self):
+        self.close()
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.nparam, np.float32)
+        check(lib.nvshmemx_mlp_get_params(self.h, p.ctypes.data), "mlp_get_params")
+        return p
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, np.float32)
+        check(lib.nvshmemx_mlp_set_params(self.h, p.ctypes.data), "mlp_set_params")
+
+    def set_normalization(self, mean, std):
+        m = np.ascontiguousarray(mean, np.float32)
+        s = np.ascontiguousarray(std, np.float32)
+        check(lib.nvshmemx_mlp_set_normalization(self.h, m.ctypes.data, s.ctypes.data), "mlp_norm")
+
+    def forward(self, X):
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.zeros((len(X), NV), np.float32)
+        check(lib.nvshmemx_mlp_forward(self.h, X.ctypes.data, len(X), Y.ctypes.data), "mlp_forward")
+        return Y
+
+    def loss_grad(self, X, Y, M):
+        X, Y, M = (np.ascontiguousarray(a, np.float32) for a in (X, Y, M))
+        loss = c_float(0)
+        g = np.zeros(self.nparam, np.float32)
+        check(lib.nvshmemx_mlp_loss_grad(self.h, X.ctypes.data, Y.ctypes.data, M.ctypes.data, len(X), byref(loss),
+                                         g.ctypes.data), "mlp_loss_grad")
+        return loss.value, g
+
+    def train(self, X, Y, M, epochs=300, batch=128, lr=2e-3, seed=1):
+        X, Y, M = (np.ascontiguousarray(a, np.float32) for a in (X, Y, M))
+        curve = np.zeros(epochs, np.float32)
+        check(lib.nvshmemx_mlp_train(self.h, X.ctypes.data, Y.ctypes.data, M.ctypes.data, len(X), epochs, batch,
+                                     lr, seed, curve.ctypes.data), "mlp_train")
+        return curve
+
+    def pick(self, X):
+        X = np.ascontiguousarray(X, np.float32)
+        v = np.zeros(len(X), np.int32)
+        mg = np.zeros(len(X), np.float32)
+        check(lib.nvshmemx_mlp_pick(self.h, X.ctypes.data, len(X), v.ctypes.data, mg.ctypes.data), "mlp_pick")
+        return v, mg
+
+
+def targets(T):
+    """log2(time in us) with a mask for variants that did not run."""
+    M = np.isfinite(T).astype(np.float32)
+    Y = np.where(M > 0, np.log2(np.maximum(np.nan_to_num(T, nan=1.0), 1e-6) * 1e3), 0.0).astype(np.float32)
+    return Y, M
+
+
+class Picker:
+    """MLP picker with the measured table as fallback."""
+
+    def __init__(self, train_x, train_t, seed=0):
+        self.tx = np.asarray(train_x, np.float32)
+        self.tt = np.asarray(train_t)
+        self.mean = self.tx.mean(0)
+        self.std = np.maximum(self.tx.std(0), 1e-3)
+        self.lo, self.hi = self.tx.min(0), self.tx.max(0)
+        self.mlp = MLP(seed)
+        self.mlp.set_normalization(self.mean, self.std)
+        self.curve = None
+
+    def fit(self, epochs=400, batch=128, lr=2e-3, seed=1):
+        Y, M = targets(self.tt)
+        self.curve = self.mlp.train(self.tx, Y, M, epochs, batch, lr, seed)
+        return self.curve
+
+    def table_pick(self, X):
+        """Best measured variant of the nearest training class."""
+        z = (np.asarray(X, np.float32) - self.mean) / self.std
+        zt = (self.tx - self.mean) / self.std
+        d = ((z[:, None, :] - zt[None, :, :]) ** 2).sum(-1)
+        nn = d.argmin(1)
+        return np.array([int(np.nanargmin(self.tt[i])) for i in nn]), nn
+
+    def pick(self, X):
+        """MLP choice; the table's where a feature leaves the training range."""
+        X = np.asarray(X, np.float32)
+        v, _ = self.mlp.pick(X)
+        out_of_range = np.any((X < self.lo - 1e-6) | (X > self.hi + 1e-6), axis=1)
+        tv, _ = self.table_pick(X)
+        return np.where(out_of_range, tv, v), out_of_range
+
+
+def regret(T, picks, mix_of):
+    """Per mix: sum of picked times / sum of best times - 1."""
+    best = np.nanmin(T, axis=1)
+    chosen = np.array([T[i, p] if np.isfinite(T[i, p]) else np.nanmax(T[i]) for i, p in enumerate(picks)])
+    out = []
+    for m in np.unique(mix_of):
+        sel = mix_of == m
+        out.append(chosen[sel].sum() / best[sel].sum() - 1.0)
+    return np.array(out)
+
+
+def evaluate(data: str = DATA, epochs=400, seed=0):
+    d = np.load(data)
+    pk = Picker(d["train_x"], d["train_t"], seed=seed)
+    curve = pk.fit(epochs=epochs)
+    hx, ht, mix = d["held_x"], d["held_t"], d["mix_of"]
+    mlp_v, oor = pk.pick(hx)
+    tab_v, _ = pk.table_pick(hx)
+    res = {
+        "mlp": regret(ht, mlp_v, mix),
+        "table": regret(ht, tab_v, mix),
+        "default_variant": regret(ht, np.full(len(hx), DEFAULT_VARIANT), mix),
+        "percall_thread": regret(ht, np.zeros(len(hx), int), mix),
+    }
+    summary = {k: {"mean_regret_pct": round(100 * float(v.mean()), 2), "max_regret_pct": round(100 * float(v.max()), 2)}
+               for k, v in res.items()}
+    summary["train_loss_first_last"] = [float(curve[0]), float(curve[-1])]
+    summary["held_out_classes"] = int(len(hx))
+    summary["fallback_used"] = int(oor.sum())
+    return summary, res, pk
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("cmd", choices=["sweep", "evaluate"])
+    ap.add_argument("--out", default=DATA)
+    ap.add_argument("--data", default=DATA)
+    ap.add_argument("--n-train", type=int, default=600)
+    ap.add_argument("--reps", type=int, default=3)
+    a = ap.parse_args()
+    if a.cmd == "sweep":
+        os.makedirs(os.path.dirname(a.out), exist_ok=True)
+        sweep(a.out, n_train=a.n_train, reps=a.reps)
+        print(json.dumps({"written": a.out}))
+    else:
+        summary, _, _ = evaluate(a.data)
+        print(json.dumps(summary))
+
+
+if __name__ == "__main__":
+    main()
