@@ -239,9 +239,10 @@ struct DevArr {
   }
 };
 
+// Device copy of a host array; h == nullptr only allocates (an output).
 static int upload(DevArr &a, const void *h, size_t bytes) {
   if (cudaMalloc(&a.p, bytes ? bytes : 4) != cudaSuccess) return fail(NVSHMEMX_ERR_NOMEM, "mlp: cudaMalloc");
-  if (bytes) return check_cuda(cudaMemcpy(a.p, h, bytes, cudaMemcpyHostToDevice), "mlp: upload");
+  if (bytes && h) return check_cuda(cudaMemcpy(a.p, h, bytes, cudaMemcpyHostToDevice), "mlp: upload");
   return 0;
 }
 

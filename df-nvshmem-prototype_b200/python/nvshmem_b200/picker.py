@@ -168,6 +168,7 @@ class MLP:
 
     def __init__(self, seed: int = 0):
         self.h = c_void_p(0)
+        lib.nvshmemx_set_error_mode(L.ERRORS_RETURN)
         check(lib.nvshmemx_mlp_create(seed, byref(self.h)), "mlp_create")
         self.nparam = lib.nvshmemx_mlp_num_params()
 

@@ -1,0 +1,100 @@
+"""The %globaltimer trace ring with its CSV export in the prototype's
+processed-trace format, and the SPMD host threads that stand in for the
+prototype's MPI processes (per-thread my_pe, per-PE allocation tails, host and
+offload barriers, and a PE thread that leaves early failing the barrier
+instead of hanging it)."""
+import ctypes
+import os
+import threading
+
+import numpy as np
+import pytest
+
+from nvshmem_b200 import ERR_STATE, _lib as L
+
+pytestmark = pytest.mark.gpu
+
+lib = L.lib
+
+
+def test_trace_ring_records_and_csv(shmem_factory, tmp_path):
+    sh = shmem_factory(2, 1 << 20)
+    flag = sh.alloc(4)
+    data = sh.alloc(1024)
+    sh.trace_enable(4096)
+    sh.pingpong(flag, data, 64, 50, skip=0)
+    assert sh.status() == 0
+    rec0, dropped0 = sh.trace_read(0)
+    rec1, _ = sh.trace_read(1)
+    assert dropped0 == 0
+    # PE 0 per iteration: one int put (256 B), one int p (recorded as put_int
+    # of one element, as the prototype does) and one wait
+    assert ((rec0["op"] == 0) & (rec0["bytes"] == 256)).sum() == 50
+    assert ((rec0["op"] == 0) & (rec0["bytes"] == 4)).sum() == 50
+    assert (rec0["op"] == 6).sum() == 50  # wait_int
+    assert (rec1["op"] == 6).sum() == 50
+    assert np.all(np.diff(rec0["t_ns"]) >= 0)
+    assert np.all(rec0["pe"] == 0) and np.all(rec1["pe"] == 1)
+    prefix = str(tmp_path / "trace")
+    sh.trace_write_csv(prefix)
+    lines = open(prefix + "_0").read().splitlines()
+    assert lines[0] == ("# timestamp, gridid, blockid, tid, type, local_address, remote_address, size, remote_pe, "
+                        "timespent")
+    row = [x.strip() for x in lines[1].split(",")]
+    assert len(row) == 10 and row[4] in ("put_int", "wait_int", "put_float")
+    assert len(lines) - 1 == len(rec0)
+    # a small ring keeps the newest records and counts the dropped ones
+    sh.trace_enable(16)
+    sh.pingpong(flag, data, 0, 40, skip=0)
+    sh.status()
+    rec, dropped = sh.trace_read(0)
+    assert len(rec) == 16 and dropped == 40 * 2 - 16
+    sh.trace_disable()
+
+
+CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p)
+
+
+def test_spmd_threads(shmem_factory):
+    npes = 4
+    sh = shmem_factory(npes, 1 << 20)
+    seen, lock = [], threading.Lock()
+    base = lib.nvshmemx_arena_base()
+    stride = lib.nvshmemx_slice_stride()
+
+    def body(_):
+        pe = lib.nvshmem_my_pe()
+        a = lib.nvshmalloc(100 + 0)
+        b = lib.nvshmalloc(28)
+        lib.nvshmem_barrier_all()
+        lib.nvshmem_barrier_all_offload()
+        lib.nvshmem_barrier_all()
+        with lock:
+            seen.append((pe, a, b))
+
+    cb = CB(body)
+    assert lib.nvshmemx_spmd_run(cb, None) == 0
+    assert sorted(p for p, _, _ in seen) == list(range(npes))
+    for pe, a, b in seen:
+        assert a == base + pe * stride and b == a + 100  # per-PE tail, no padding
+    assert sh.status() == 0
+
+
+def test_spmd_departed_pe_fails_barrier(shmem_factory):
+    os.environ["NVSHMEM_HOST_BARRIER_TIMEOUT_S"] = "20"
+    sh = shmem_factory(3, 1 << 20)
+    results, lock = [], threading.Lock()
+
+    def body(_):
+        pe = lib.nvshmem_my_pe()
+        if pe == 1:
+            return  # this PE leaves without reaching the barrier
+        lib.nvshmem_barrier_all()
+        with lock:
+            results.append(pe)
+
+    cb = CB(body)
+    rc = lib.nvshmemx_spmd_run(cb, None)
+    assert rc == ERR_STATE
+    assert sorted(results) == [0, 2]  # both returned (with an error) instead of hanging
+    assert sh.status() == ERR_STATE
