@@ -223,6 +223,109 @@ def run_extras(peak):
     return out
 
 
+def run_c1_sweep():
+    """C1 put sweep: PE 0 puts 4 B .. 1 MiB of float32 payload (uniform in
+    [-1, 1), seed 0) to PE 1 with one call: nvshmem_float_put by one thread
+    (the prototype's shape), and the CTA and CTA-TMA cooperative forms.  Each
+    figure is one launch with one request (launch overhead included)."""
+    import numpy as np
+    from nvshmem_b200 import DT_FLOAT, MODE_BLOCK, MODE_BULK, MODE_THREAD, REQ_PUT, REQUEST_DTYPE, Shmem
+    from nvshmem_b200.traffic import c1_float_payload, c1_sizes
+    heap = 8 << 20
+    out = {}
+    with Shmem(2, heap) as sh:
+        payload = c1_float_payload((1 << 20) // 4, seed=0)
+        sh.write(0, 0, payload)
+        for size in c1_sizes():
+            r = np.zeros(1, REQUEST_DTYPE)
+            r[0] = (0, 4 << 20, size, 0, 1, REQ_PUT, DT_FLOAT, 0, 0)
+            row = {}
+            for mode, name in ((MODE_THREAD, "thread"), (MODE_BLOCK, "cta"), (MODE_BULK, "cta_tma")):
+                sh.exec_requests(r, mode)
+                ts = sorted(sh.exec_requests(r, mode) for _ in range(5))
+                us = 1e3 * ts[2]
+                row[name] = {"us": round(us, 2), "GBps": round(2 * size / (us * 1e-6) / 1e9, 2)}
+            assert sh.compare(1, 4 << 20, 0, 0, size) == 0
+            out[str(size)] = row
+        assert sh.status() == 0
+    return out
+
+
+def run_c2_sweep(peak):
+    """C2 all-to-all on 8 PEs across message sizes and element types: each
+    round every PE puts (or gets) one message to (from) each of the 7 others,
+    then quiet + device barrier; buffer sets rotate so large working sets
+    exceed 2x L2.  Bit-exactness is checked on the device after each size."""
+    from nvshmem_b200 import DT_DOUBLE, DT_FLOAT, DT_INT, MODE_BULK, REQ_GET, REQ_PUT, Shmem
+    out = {}
+    plan = [(8, DT_INT), (512, DT_FLOAT), (32 << 10, DT_DOUBLE), (1 << 20, DT_FLOAT), (16 << 20, DT_INT),
+            (256 << 20, DT_DOUBLE)]
+    for nbytes, dt in plan:
+        nsets = max(1, min(8, (512 << 20) // (2 * 8 * 8 * nbytes)))
+        heap = 2 * 8 * nbytes * nsets
+        heap = max(heap, 1 << 20)
+        rounds = max(nsets, min(400, int(4e9 // max(112 * nbytes, 1))))
+        with Shmem(8, heap) as sh:
+            for pe in range(8):
+                sh.fill_random(pe, 0, heap, 1)
+            row = {}
+            for op, name in ((REQ_PUT, "put"), (REQ_GET, "get")):
+                kw = dict(rounds=rounds, nsets=nsets, set_stride=16 * nbytes, mode=MODE_BULK, ctas_per_pe=18)
+                sh.alltoall(op, dt, 0, 8 * nbytes, nbytes, **dict(kw, rounds=nsets))
+                ms = sh.alltoall(op, dt, 0, 8 * nbytes, nbytes, **kw)
+                gbs = 2 * 8 * 7 * nbytes * rounds / (ms / 1e3) / 1e9
+                row[name] = {"GBps": round(gbs, 1), "frac": round(gbs / peak, 3), "us_per_round": round(1e3 * ms / rounds, 2)}
+            for p in range(8):
+                for q in range(8):
+                    if p != q:
+                        assert sh.compare(q, 8 * nbytes + p * nbytes, p, q * nbytes, nbytes) == 0
+            assert sh.status() == 0
+        out[f"{nbytes}B_dt{dt}"] = row
+    return out
+
+
+def run_c3_halo(peak):
+    """C3: 8 PEs on a periodic 2x2x2 grid, 256^3 float64 per PE, 100
+    iterations of 6 face puts (x faces gathered with stride 256) + int_p
+    signals + int_wait + device barrier."""
+    from nvshmem_b200 import Shmem
+    n, iters = 256, 100
+    block, ghosts = n ** 3 * 8, 6 * n * n * 8
+    heap = block + ghosts + 4096
+    with Shmem(8, heap) as sh:
+        for pe in range(8):
+            sh.fill_random(pe, 0, block, 3)
+            sh.memset(pe, block, 0, ghosts + 4096)
+        sh.halo(2, 2, 2, n, 0, block, block + ghosts, 3, 18)
+        for pe in range(8):
+            sh.memset(pe, block + ghosts, 0, 64)
+        ms = sh.halo(2, 2, 2, n, 0, block, block + ghosts, iters, 18)
+        assert sh.status() == 0
+    face_bytes = 8 * 6 * n * n * 8
+    return {"us_per_iter": round(1e3 * ms / iters, 2), "face_GBps": round(2 * face_bytes * iters / (ms / 1e3) / 1e9, 1),
+            "iters": iters, "n": n}
+
+
+def run_c5_picker():
+    from nvshmem_b200 import picker
+    if not os.path.exists(picker.DATA):
+        return {"unavailable": "no variant timings measured"}
+    summary, _, _ = picker.evaluate(picker.DATA, epochs=400)
+    return summary
+
+
+def cpu_latency():
+    from oracle import model as om
+    if not os.path.exists(om.HOST_BENCH):
+        om.build()
+    pp = json.loads(subprocess.run([om.HOST_BENCH, "pingpong", "10000"], capture_output=True, text=True,
+                                   timeout=300, check=True).stdout.strip().splitlines()[-1])
+    br = json.loads(subprocess.run([om.HOST_BENCH, "barrier", "8", "10000"], capture_output=True, text=True,
+                                   timeout=300, check=True).stdout.strip().splitlines()[-1])
+    return {"pingpong_rtt_ns_p50": pp["p50_ns"], "barrier_8_ns_p50": br["p50_ns"], "cores": br["cores"],
+            "kind": "port"}
+
+
 def run_gpu(args, rank, world, local):
     import numpy as np
     import torch
@@ -298,6 +401,10 @@ def run_gpu(args, rank, world, local):
             checks = [sh.checksum(pe, 0, C4["heap"]) for pe in range(C4["npes"])]
         if args.only != "batch":
             out.update(run_extras(peak))
+            out["c1_float_put_sweep"] = run_c1_sweep()
+            out["c2_alltoall_sweep"] = run_c2_sweep(peak)
+            out["c3_halo"] = run_c3_halo(peak)
+            out["c5_picker_regret"] = run_c5_picker()
     clocks = sampler.summary()
 
     value = world * alg * args.steps / t_batch / 1e9
@@ -331,6 +438,8 @@ def run_gpu(args, rank, world, local):
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = {k: v for k, v in cpu_baseline(reqs, C4["npes"], C4["heap"]).items()
                                 if k in ("value", "unit", "cores", "kind", "sample")}
+        if args.only != "batch":
+            line["cpu_latency"] = cpu_latency()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
