@@ -430,7 +430,9 @@ def run_gpu(args, rank, world, local):
         "gpu_launches": 2 * args.steps * 2,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 3), "traffic": traffic,
-                     "kernel": "batch_exec_kernel", "peak_kind": peak_kind},
+                     "kernel": ("batch_exec_tma_kernel" if cfg_used.get("tma_stages") else "batch_exec_kernel"),
+                     "peak_kind": peak_kind, "alg_bytes_per_launch": alg,
+                     "traffic_source": "profiles/batch_exec_c4.json (ncu, full size, 1 pass)"},
         "clocks": clocks,
         "heap_checksum": int(sum(checks) % (1 << 64)),
     }
