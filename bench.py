@@ -196,9 +196,10 @@ def run_extras(peak):
     with Shmem(8, 1 << 20) as sh:
         bar = {}
         for ctas in (1, 16):
-            ns, _ = sh.barrier_latency(ctas, 10000)
-            bar[f"{ctas}_cta_per_pe"] = {"p50": round(float(np.percentile(ns, 50)), 1),
-                                         "p99": round(float(np.percentile(ns, 99)), 1)}
+            for counted, kind in ((False, "ticket"), (True, "counted")):
+                ns, _ = sh.barrier_latency(ctas, 10000, counted)
+                bar[f"{kind}_{ctas}_cta_per_pe"] = {"p50": round(float(np.percentile(ns, 50)), 1),
+                                                    "p99": round(float(np.percentile(ns, 99)), 1)}
         out["barrier_ns"] = bar
         out["offload_barrier_us_per_call"] = round(sh.offload_barrier(1000), 3)
     # C2 bulk all-to-all: 8 PEs, 1 MiB and 16 MiB messages, rotating sets > 2x L2

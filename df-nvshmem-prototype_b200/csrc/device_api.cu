@@ -269,6 +269,16 @@ __device__ int nvshmemx_barrier_all(void) {
 }
 __device__ int nvshmemx_barrier_pe(void) { return nvshm::barrier_pe(CFG); }
 
+__device__ int nvshmemx_barrier_all_ep(unsigned long long episode) {
+  const Cfg &c = CFG;
+  unsigned long long t0 = c.trace ? nvshm::gtimer() : 0;
+  const unsigned long long P = (unsigned long long)gridDim.x * gridDim.y * gridDim.z;
+  int rc = nvshm::episode_barrier(c, c.coll_bar, P, episode);
+  if (c.trace && nvshm::block_rank() == 0)
+    nvshm::trace_rec(c, NVSHMEMX_TRACE_BARRIER, nullptr, nullptr, 0, nvshm::my_pe(), t0, nvshm::gtimer());
+  return rc;
+}
+
 }  // extern "C"
 
 namespace nvshm {

@@ -250,12 +250,15 @@ __global__ void pingpong_kernel(int *data, int *flag, int len, int iters, int sk
 }
 
 // ------------------------------------------------------------ barrier latency
-__global__ void barrier_latency_kernel(int iters, long long *cycles, unsigned long long *gt) {
+__global__ void barrier_latency_kernel(int iters, int counted, long long *cycles, unsigned long long *gt) {
   const bool rec = blockIdx.x == 0 && blockIdx.z == 0 && threadIdx.x == 0;
   unsigned long long g0 = nvshm::gtimer();
   long long t = clock64();
   for (int i = 0; i < iters; ++i) {
-    nvshmemx_barrier_all();
+    if (counted)
+      nvshmemx_barrier_all_ep((unsigned long long)i);
+    else
+      nvshmemx_barrier_all();
     if (rec) {
       long long t1 = clock64();
       cycles[i] = t1 - t;
@@ -336,7 +339,7 @@ __global__ void alltoall_kernel(Cfg c, int op, int dtype, unsigned long long sen
       }
     }
     nvshmem_quiet();
-    nvshmemx_barrier_all();
+    nvshmemx_barrier_all_ep((unsigned long long)r);
   }
 }
 
@@ -391,7 +394,7 @@ __global__ void halo_kernel(Cfg c, int px, int py, int pz, int n, unsigned long 
       nvshmem_int_p((int *)(c.arena + sig_off) + (d ^ 1), it + 1, halo_nbr(pe, d, px, py, pz));
       nvshmem_int_wait_until(my_sig + d, 0, it + 1);
     }
-    nvshmemx_barrier_all();
+    nvshmemx_barrier_all_ep((unsigned long long)it);
   }
 }
 
@@ -554,14 +557,14 @@ int nvshmemx_op_pingpong(size_t flag_off, size_t data_off, int len_elems, int it
   return 0;
 }
 
-int nvshmemx_op_barrier_latency(int ctas_per_pe, int iters, double *out_ns, double *out_total_ns) {
+int nvshmemx_op_barrier_latency(int ctas_per_pe, int iters, int counted, double *out_ns, double *out_total_ns) {
   int rc;
   if ((rc = need_started())) return rc;
   if (ctas_per_pe < 1 || iters < 1) return fail(NVSHMEMX_ERR_INVALID, "barrier_latency: bad arguments");
   long long *cyc = (long long *)g_out_buf.get((size_t)iters * 8 + 64);
   if (!cyc) return fail(NVSHMEMX_ERR_NOMEM, "barrier scratch");
   unsigned long long *gt = (unsigned long long *)(cyc + iters);
-  void *args[] = {&iters, &cyc, &gt};
+  void *args[] = {&iters, &counted, &cyc, &gt};
   if ((rc = launch_collective((const void *)barrier_latency_kernel, dim3(ctas_per_pe), dim3(128), args, 0, 0)))
     return rc;
   if ((rc = check_cuda(cudaDeviceSynchronize(), "barrier_latency"))) return rc;

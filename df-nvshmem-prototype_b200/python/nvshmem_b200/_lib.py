@@ -108,7 +108,7 @@ _SIGS = {
     "nvshmemx_compare": (c_int, [c_int, c_size_t, c_int, c_size_t, c_size_t, _P(c_ulonglong)]),
     "nvshmemx_checksum": (c_int, [c_int, c_size_t, c_size_t, _P(c_ulonglong)]),
     "nvshmemx_op_pingpong": (c_int, [c_size_t, c_size_t, c_int, c_int, c_int, _P(c_double), _P(c_double)]),
-    "nvshmemx_op_barrier_latency": (c_int, [c_int, c_int, _P(c_double), _P(c_double)]),
+    "nvshmemx_op_barrier_latency": (c_int, [c_int, c_int, c_int, _P(c_double), _P(c_double)]),
     "nvshmemx_op_offload_barrier": (c_int, [c_int, _P(c_double)]),
     "nvshmemx_op_alltoall": (c_int, [c_int, c_int, c_size_t, c_size_t, c_size_t, c_int, c_int,
                                      c_size_t, c_int, c_int, _P(c_float)]),

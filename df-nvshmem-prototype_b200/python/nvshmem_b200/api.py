@@ -106,10 +106,10 @@ class Shmem:
               "pingpong")
         return out, total.value
 
-    def barrier_latency(self, ctas_per_pe, iters):
+    def barrier_latency(self, ctas_per_pe, iters, counted=False):
         out = np.zeros(iters, dtype=np.float64)
         total = c_double(0)
-        check(lib.nvshmemx_op_barrier_latency(ctas_per_pe, iters,
+        check(lib.nvshmemx_op_barrier_latency(ctas_per_pe, iters, int(counted),
                                               out.ctypes.data_as(ctypes.POINTER(c_double)),
                                               byref(total)), "barrier_latency")
         return out, total.value

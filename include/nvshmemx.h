@@ -210,6 +210,11 @@ __device__ int nvshmemx_int_wait_until_cmp(int *ivar, int cmp, int value, long l
 __device__ int nvshmemx_barrier_all(void);
 /* Barrier over the CTAs of the calling PE only. */
 __device__ int nvshmemx_barrier_pe(void);
+/* nvshmemx_barrier_all for callers that count their barriers: `episode` is
+ * the number of earlier device barriers of this collective launch (0 for the
+ * first).  Every CTA must pass the same sequence.  Saves one atomic round
+ * trip per barrier. */
+__device__ int nvshmemx_barrier_all_ep(unsigned long long episode);
 #ifdef __cplusplus
 }
 #endif

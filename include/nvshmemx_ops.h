@@ -89,10 +89,11 @@ int nvshmemx_op_pingpong(size_t flag_off, size_t data_off, int len_elems, int it
                          double *out_ns, double *out_total_ns);
 
 /* ---- device barrier latency --------------------------------------------- */
-/* iters back-to-back nvshmemx_barrier_all() over ctas_per_pe CTAs per PE;
- * out_ns[iters] = per-barrier interval seen by PE 0's first CTA (may be
- * NULL), *out_total_ns the total. */
-int nvshmemx_op_barrier_latency(int ctas_per_pe, int iters, double *out_ns, double *out_total_ns);
+/* iters back-to-back device barriers over ctas_per_pe CTAs per PE:
+ * nvshmemx_barrier_all() (counted == 0) or nvshmemx_barrier_all_ep(i)
+ * (counted != 0); out_ns[iters] = per-barrier interval seen by PE 0's first
+ * CTA (may be NULL), *out_total_ns the total. */
+int nvshmemx_op_barrier_latency(int ctas_per_pe, int iters, int counted, double *out_ns, double *out_total_ns);
 /* iters host calls of nvshmem_barrier_all_offload(); *out_us_per_call. */
 int nvshmemx_op_offload_barrier(int iters, double *out_us_per_call);
 

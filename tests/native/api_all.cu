@@ -54,6 +54,7 @@ __global__ void every_device_call(int *ia, float *fa, double *da, char *smem_unu
   nvshmemx_int_wait_until_cmp(li, NVSHMEMX_CMP_GE, 1, 1000);
   nvshmemx_barrier_pe();
   nvshmemx_barrier_all();
+  nvshmemx_barrier_all_ep(1);
   nvshmem_trace_end();
 }
 

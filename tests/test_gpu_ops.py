@@ -43,10 +43,11 @@ def test_pingpong_flag_only_latency(shmem_factory):
     assert 0 < p50 < 50_000  # a round trip through L2, far below 50 us
 
 
+@pytest.mark.parametrize("counted", [False, True])
 @pytest.mark.parametrize("ctas", [1, 4])
-def test_barrier_latency(shmem_factory, ctas):
+def test_barrier_latency(shmem_factory, ctas, counted):
     sh = shmem_factory(8, 1 << 20)
-    ns, total = sh.barrier_latency(ctas, 2000)
+    ns, total = sh.barrier_latency(ctas, 2000, counted)
     assert sh.status() == 0
     assert 0 < np.median(ns) < 100_000
 
