@@ -405,7 +405,9 @@ __device__ __forceinline__ int ticket_barrier(const Cfg &c, unsigned long long *
   __syncthreads();
   int rc = 0;
   if (block_rank() == 0) {
-    __threadfence();
+    // bar.sync orders the CTA's earlier writes before this thread's
+    // operations; the acq_rel atomic releases them at GPU scope (cumulative),
+    // so no separate fence is needed.
     const unsigned long long t = atom_add_acq_rel_u64(ctr, 1ull);
     const unsigned long long target = (t / P + 1ull) * P;
     if (ld_acquire_u64(ctr) < target) {
@@ -440,8 +442,7 @@ __device__ __forceinline__ int episode_barrier(const Cfg &c, unsigned long long 
   __syncthreads();
   int rc = 0;
   if (block_rank() == 0) {
-    __threadfence();
-    red_add_release_u64(ctr, 1ull);
+    red_add_release_u64(ctr, 1ull);  // releases the CTA's writes (see ticket_barrier)
     const unsigned long long target = (episode + 1ull) * P;
     if (ld_acquire_u64(ctr) < target) {
       const unsigned long long t0 = gtimer();

@@ -338,7 +338,10 @@ __global__ void alltoall_kernel(Cfg c, int op, int dtype, unsigned long long sen
         b += len;
       }
     }
-    nvshmem_quiet();
+    // quiet + barrier: the barrier's __syncthreads orders every thread's
+    // stores before the leader, whose quiet and release cover them all
+    __syncthreads();
+    if (threadIdx.x == 0) nvshmem_quiet();
     nvshmemx_barrier_all_ep((unsigned long long)r);
   }
 }
