@@ -195,22 +195,14 @@ __global__ void __launch_bounds__(1024) batch_exec_kernel(const WorkItem *__rest
 }
 
 // ------------------------------------------------------- exec through TMA
-// Same claiming loop as batch_exec_kernel, but the 16-byte-aligned body of
-// every copy chunk goes through a per-warp ring of S shared-memory stages:
-// lane 0 issues cp.async.bulk global->shared (completion counted on the
-// stage's mbarrier) and, once a stage has landed, cp.async.bulk
-// shared->global as one bulk group.  The ring spans work items, so each warp
-// keeps up to S loads in flight across chunk boundaries without holding the
-// data in registers; lanes 1..31 copy the unaligned head and tail bytes.
-// Chunks whose source and destination differ in alignment modulo 16, or that
-// are shorter than min_bulk, take the register copy.
-struct WarpRing {
-  unsigned long long *mbar;  // S mbarriers
-  unsigned long long *pdst;  // destination of the piece in each stage
-  unsigned *plen;            // length of the piece in each stage
-  char *buf;                 // S * SB bytes
-};
-
+// A per-warp ring of S shared-memory stages: lane 0 issues cp.async.bulk
+// global->shared (completion counted on the stage's mbarrier) and, once a
+// stage has landed, cp.async.bulk shared->global as one bulk group.  The ring
+// spans work items, so each warp keeps up to S loads in flight across chunk
+// boundaries without holding the data in registers; lanes 1..31 copy the
+// unaligned head and tail bytes.  Chunks whose source and destination differ
+// in alignment modulo 16, or that are shorter than min_bulk, take the
+// register copy.  Every mbarrier wait is bounded by `deadline`.
 __device__ __forceinline__ void bulk_wait_read_le(unsigned n) {
   switch (n) {
     case 0: asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); break;
@@ -221,39 +213,106 @@ __device__ __forceinline__ void bulk_wait_read_le(unsigned n) {
 }
 
 template <int S>
+struct WarpTma {
+  unsigned long long *mbar;  // S mbarriers
+  unsigned long long *pdst;  // destination of the piece in each stage
+  unsigned *plen;            // length of the piece in each stage
+  char *buf;                 // S * SB bytes
+  unsigned SB, min_bulk;
+  unsigned issued, retired;  // pieces (lane 0's view)
+  bool ok;
+  unsigned long long deadline;
+
+  // Per-warp region: 256 bytes of mbarriers and piece records, then the stages.
+  __device__ __forceinline__ void init(char *smem, unsigned stage_bytes, unsigned minb, long long timeout_ns,
+                                       unsigned lane) {
+    const unsigned warp = threadIdx.x >> 5;
+    char *base = smem + (size_t)warp * (256 + (size_t)S * stage_bytes);
+    mbar = reinterpret_cast<unsigned long long *>(base);
+    pdst = reinterpret_cast<unsigned long long *>(base + 64);
+    plen = reinterpret_cast<unsigned *>(base + 128);
+    buf = base + 256;
+    SB = stage_bytes;
+    min_bulk = minb;
+    issued = retired = 0;
+    ok = true;
+    deadline = gtimer() + (unsigned long long)timeout_ns;
+    if (lane == 0) {
+      for (int s = 0; s < S; ++s) mbar_init(mbar + s, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncwarp();
+  }
+
+  // lane 0: wait for the oldest piece to land, then store it from its stage
+  __device__ __forceinline__ void retire_one() {
+    const unsigned p = retired, s = p % S;
+    if (ok && !mbar_wait(mbar + s, (p / S) & 1u, deadline)) ok = false;
+    if (ok) {
+      bulk_s2g(reinterpret_cast<void *>(pdst[s]), buf + (size_t)s * SB, plen[s]);
+      bulk_commit();
+    }
+    ++retired;
+  }
+
+  // One work item, all lanes of the warp.
+  __device__ __forceinline__ void run(const WorkItem &w, unsigned lane) {
+    char *d = reinterpret_cast<char *>(w.dst);
+    const char *s = reinterpret_cast<const char *>(w.src);
+    if (w.kind != kCopy || (((uintptr_t)d ^ (uintptr_t)s) & 15) != 0 || w.len < min_bulk) {
+      run_item<16, 4>(w, lane);
+      return;
+    }
+    unsigned head = (unsigned)((16 - ((uintptr_t)d & 15)) & 15);
+    if (head > w.len) head = w.len;
+    const unsigned body = (w.len - head) & ~15u;
+    const unsigned tail = w.len - head - body;
+    if (lane != 0) {
+      for (unsigned i = lane - 1; i < head; i += 31) d[i] = s[i];
+      for (unsigned i = lane - 1; i < tail; i += 31) d[head + body + i] = s[head + body + i];
+    } else if (ok) {
+      for (unsigned off = 0; off < body && ok; off += SB) {
+        const unsigned len = body - off < SB ? body - off : SB;
+        if (issued - retired == (unsigned)S) retire_one();
+        const unsigned st = issued % S;
+        // the store that last read this stage (piece issued - S) must be
+        // done reading: at most `after` younger stores may still be pending
+        if (issued >= (unsigned)S) bulk_wait_read_le(retired - 1u - (issued - (unsigned)S));
+        pdst[st] = (unsigned long long)(d + head + off);
+        plen[st] = len;
+        mbar_expect_tx(mbar + st, len);
+        bulk_g2s(buf + (size_t)st * SB, s + head + off, len, mbar + st);
+        ++issued;
+      }
+    }
+    __syncwarp();
+  }
+
+  // lane 0: store what is still in flight and wait for every store.
+  // Returns false if an mbarrier wait passed the deadline.
+  __device__ __forceinline__ bool drain(unsigned lane) {
+    if (lane == 0) {
+      while (retired < issued) retire_one();
+      bulk_wait_all();
+      if (ok)
+        for (int s = 0; s < S; ++s) mbar_inval(mbar + s);
+    }
+    return __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+  }
+};
+
+template <int S>
 __global__ void __launch_bounds__(256) batch_exec_tma_kernel(const WorkItem *__restrict__ items, BatchCtl *ctl,
                                                               unsigned long long cap, int grab, unsigned SB,
                                                               unsigned min_bulk, long long timeout_ns) {
   extern __shared__ __align__(128) char smem[];
-  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  char *base = smem + (size_t)warp * (256 + (size_t)S * SB);
-  WarpRing ring;
-  ring.mbar = reinterpret_cast<unsigned long long *>(base);
-  ring.pdst = reinterpret_cast<unsigned long long *>(base + 64);
-  ring.plen = reinterpret_cast<unsigned *>(base + 128);
-  ring.buf = base + 256;
+  const unsigned lane = threadIdx.x & 31u;
   if (*(volatile int *)&ctl->status != 0) return;
   const unsigned long long C = *(volatile unsigned long long *)&ctl->total_chunks;
   if (C > cap) return;
-  unsigned issued = 0, retired = 0;
-  bool ok = true;
-  const unsigned long long deadline = gtimer() + (unsigned long long)timeout_ns;
-  if (lane == 0) {
-    for (int s = 0; s < S; ++s) mbar_init(ring.mbar + s, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  }
-  __syncwarp();
-  // lane 0: wait for the oldest piece to land, then store it from its stage
-  auto retire_one = [&]() {
-    const unsigned p = retired, s = p % S;
-    if (ok && !mbar_wait(ring.mbar + s, (p / S) & 1u, deadline)) ok = false;
-    if (ok) {
-      bulk_s2g(reinterpret_cast<void *>(ring.pdst[s]), ring.buf + (size_t)s * SB, ring.plen[s]);
-      bulk_commit();
-    }
-    ++retired;
-  };
+  WarpTma<S> ring;
+  ring.init(smem, SB, min_bulk, timeout_ns, lane);
   unsigned long long bse = 0;
   if (lane == 0) bse = atomicAdd(&ctl->cursor, (unsigned long long)grab);
   bse = __shfl_sync(0xffffffffu, bse, 0);
@@ -261,49 +320,233 @@ __global__ void __launch_bounds__(256) batch_exec_tma_kernel(const WorkItem *__r
     unsigned long long nxt = 0;
     if (lane == 0) nxt = atomicAdd(&ctl->cursor, (unsigned long long)grab);
     const unsigned long long end = bse + grab < C ? bse + grab : C;
-    for (unsigned long long k = bse; k < end; ++k) {
-      const WorkItem w = load_item(items + k);
-      char *d = reinterpret_cast<char *>(w.dst);
-      const char *s = reinterpret_cast<const char *>(w.src);
-      if (w.kind != kCopy || (((uintptr_t)d ^ (uintptr_t)s) & 15) != 0 || w.len < min_bulk) {
-        run_item<16, 4>(w, lane);
-        continue;
-      }
-      unsigned head = (unsigned)((16 - ((uintptr_t)d & 15)) & 15);
-      if (head > w.len) head = w.len;
-      const unsigned body = (w.len - head) & ~15u;
-      const unsigned tail = w.len - head - body;
-      if (lane != 0) {
-        for (unsigned i = lane - 1; i < head; i += 31) d[i] = s[i];
-        for (unsigned i = lane - 1; i < tail; i += 31) d[head + body + i] = s[head + body + i];
-      } else if (ok) {
-        for (unsigned off = 0; off < body && ok; off += SB) {
-          const unsigned len = body - off < SB ? body - off : SB;
-          if (issued - retired == (unsigned)S) retire_one();
-          const unsigned st = issued % S;
-          // the store that last read this stage (piece issued - S) must be
-          // done reading: at most `after` younger stores may still be pending
-          if (issued >= (unsigned)S) bulk_wait_read_le(retired - 1u - (issued - (unsigned)S));
-          ring.pdst[st] = (unsigned long long)(d + head + off);
-          ring.plen[st] = len;
-          mbar_expect_tx(ring.mbar + st, len);
-          bulk_g2s(ring.buf + (size_t)st * SB, s + head + off, len, ring.mbar + st);
-          ++issued;
-        }
-      }
-      __syncwarp();
-    }
+    for (unsigned long long k = bse; k < end; ++k) ring.run(load_item(items + k), lane);
     bse = __shfl_sync(0xffffffffu, nxt, 0);
   }
-  if (lane == 0) {
-    while (retired < issued) retire_one();
-    bulk_wait_all();
-    if (!ok) {
-      if (atomicCAS(&ctl->status, 0, NVSHMEMX_ERR_TIMEOUT) == 0) ctl->bad_request = -2;
-    } else {
-      for (int s = 0; s < S; ++s) mbar_inval(ring.mbar + s);
+  if (!ring.drain(lane) && lane == 0) {
+    if (atomicCAS(&ctl->status, 0, NVSHMEMX_ERR_TIMEOUT) == 0) ctl->bad_request = -2;
+  }
+}
+
+// ------------------------------------------------ streaming: one launch
+// Planning and execution in one persistent cooperative launch.  The first
+// `planners` warps of every CTA read the requests -- from device memory, or
+// straight from pinned host memory for the end-to-end call, so the transfer
+// over the host link overlaps execution -- validate and translate them 32 at
+// a time, reserve their chunks with one atomicAdd per 32 requests on
+// ctl->total_chunks and publish each work item with a release store of the
+// launch's generation number in its last word.  Every warp (planners too,
+// once their share is planned) claims chunk indices from ctl->cursor and
+// waits for the item's generation tag before running it through its TMA
+// ring.  A warp stops at the first index at or beyond the final chunk count,
+// which is known once every planner has added itself to ctl->plan_done.
+// Unlike the graph path, an invalid request is skipped on its own (and
+// reported); the valid ones still run.
+struct StreamCtl {                 // the first 32 bytes match BatchCtl
+  unsigned long long total_chunks;
+  unsigned long long cursor;
+  int status;
+  int bad_request;
+  unsigned long long pad0;
+  unsigned int plan_done;
+  unsigned int gen;                // generation of the current launch; outside
+                                   // the 32 bytes the graph path zeroes, so it
+                                   // only ever grows
+  unsigned long long pad[3];
+};
+
+__device__ __forceinline__ void plan_one(const Cfg &c, const nvshmemx_request &r, int i, unsigned chunk,
+                                         BatchCtl *ctl, WorkItem &w, unsigned &cnt) {
+  cnt = 0;
+  w.dst = w.src = 0;
+  w.len = 0;
+  w.kind = kCopy;
+  w.value = 0;
+  w.pad = 0;
+  const unsigned width = r.dtype == NVSHMEMX_DT_DOUBLE ? 8u : 4u;
+  const bool pe_ok = r.src_pe < c.npes && r.dst_pe < c.npes && r.dtype <= NVSHMEMX_DT_DOUBLE;
+  const unsigned long long dst = (unsigned long long)c.arena + ((unsigned long long)r.dst_pe << c.log2_stride) + r.dst_off;
+  const unsigned long long src = (unsigned long long)c.arena + ((unsigned long long)r.src_pe << c.log2_stride) + r.src_off;
+  switch (r.op) {
+    case NVSHMEMX_REQ_PUT:
+    case NVSHMEMX_REQ_GET:
+    case NVSHMEMX_REQ_G: {
+      const unsigned long long bytes = r.op == NVSHMEMX_REQ_G ? width : r.bytes;
+      if (!pe_ok || r.src_off + bytes > c.slice_bytes || r.dst_off + bytes > c.slice_bytes) {
+        set_status(ctl, NVSHMEMX_ERR_BOUNDS, i);
+        return;
+      }
+      w.dst = dst;
+      w.src = src;
+      w.len = (unsigned)bytes;
+      cnt = bytes ? (unsigned)((bytes + chunk - 1) / chunk) : 0u;
+      return;
+    }
+    case NVSHMEMX_REQ_SIGNAL:
+    case NVSHMEMX_REQ_P: {
+      const unsigned bytes = r.op == NVSHMEMX_REQ_SIGNAL ? 4u : width;
+      if (!pe_ok || r.dst_off + bytes > c.slice_bytes || (r.dst_off & (bytes - 1))) {
+        set_status(ctl, NVSHMEMX_ERR_BOUNDS, i);
+        return;
+      }
+      w.dst = dst;
+      w.src = r.src_off;
+      w.len = bytes;
+      w.kind = r.op == NVSHMEMX_REQ_SIGNAL ? kSignal : kStore;
+      w.value = r.value;
+      cnt = 1;
+      return;
+    }
+    default:
+      set_status(ctl, NVSHMEMX_ERR_INVALID, i);
+  }
+}
+
+__device__ __forceinline__ void publish_item(WorkItem *p, const WorkItem &w, unsigned gen) {
+  uint4 a = make_uint4((unsigned)w.dst, (unsigned)(w.dst >> 32), (unsigned)w.src, (unsigned)(w.src >> 32));
+  *reinterpret_cast<uint4 *>(p) = a;
+  uint2 b = make_uint2(w.len, w.kind);
+  *reinterpret_cast<uint2 *>(reinterpret_cast<char *>(p) + 16) = b;
+  *reinterpret_cast<int *>(reinterpret_cast<char *>(p) + 24) = w.value;
+  st_release_b32(reinterpret_cast<char *>(p) + 28, gen);
+}
+
+__device__ __forceinline__ WorkItem read_item(const WorkItem *p) {
+  const uint4 a = __ldcg(reinterpret_cast<const uint4 *>(p));
+  const uint4 b = __ldcg(reinterpret_cast<const uint4 *>(p) + 1);
+  WorkItem w;
+  w.dst = ((unsigned long long)a.y << 32) | a.x;
+  w.src = ((unsigned long long)a.w << 32) | a.z;
+  w.len = b.x;
+  w.kind = b.y;
+  w.value = (int)b.z;
+  w.pad = b.w;
+  return w;
+}
+
+__device__ __forceinline__ nvshmemx_request load_request(const nvshmemx_request *p) {
+  const uint4 a = __ldcg(reinterpret_cast<const uint4 *>(p));
+  const uint4 b = __ldcg(reinterpret_cast<const uint4 *>(p) + 1);
+  nvshmemx_request r;
+  memcpy(&r, &a, 16);
+  memcpy(reinterpret_cast<char *>(&r) + 16, &b, 16);
+  return r;
+}
+
+// 1: item k is ready; 2: there is no item k (all planning done and k is past
+// the end, or past the table); 3: the deadline passed.
+__device__ __forceinline__ int wait_item(StreamCtl *ctl, const WorkItem *items, unsigned long long k,
+                                         unsigned long long cap, unsigned gen, unsigned planners,
+                                         unsigned long long deadline) {
+  if (k >= cap) return 2;
+  const int *tag = reinterpret_cast<const int *>(reinterpret_cast<const char *>(items + k) + 28);
+  unsigned ns = 0;
+  for (unsigned spins = 0;; ++spins) {
+    if (k < ld_acquire_u64(&ctl->total_chunks)) {
+      if ((unsigned)ld_acquire(tag) == gen) return 1;
+    } else if ((unsigned)ld_acquire(reinterpret_cast<const int *>(&ctl->plan_done)) == planners) {
+      if (k >= ld_acquire_u64(&ctl->total_chunks)) return 2;
+      continue;
+    }
+    if (spins > 8) {
+      ns = ns == 0 ? 32 : (ns >= 512 ? 512 : ns * 2);
+      __nanosleep(ns);
+    }
+    if ((spins & 15) == 15 && gtimer() > deadline) return 3;
+  }
+}
+
+template <int S>
+__global__ void __launch_bounds__(256) batch_stream_kernel(Cfg c, const nvshmemx_request *reqs, int n,
+                                                           unsigned chunk, WorkItem *__restrict__ items,
+                                                           unsigned long long cap, StreamCtl *ctl, int grab,
+                                                           unsigned SB, unsigned min_bulk, int planners_per_cta) {
+  extern __shared__ __align__(128) char smem[];
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  BatchCtl *bctl = reinterpret_cast<BatchCtl *>(ctl);
+  const unsigned gen = *(volatile unsigned *)&ctl->gen;
+  const unsigned planners = gridDim.x * (unsigned)planners_per_cta;
+  WarpTma<S> ring;
+  ring.init(smem, SB, min_bulk, c.wait_timeout_ns, lane);
+  // ---- planning (the first planners_per_cta warps of each CTA)
+  if (warp < (unsigned)planners_per_cta) {
+    const unsigned me = blockIdx.x * (unsigned)planners_per_cta + warp;
+    const int ngroups = (n + 31) / 32;
+    int g = (int)me;
+    nvshmemx_request r;
+    if (g < ngroups && g * 32 + (int)lane < n) r = load_request(reqs + g * 32 + lane);
+    for (; g < ngroups; g += (int)planners) {
+      const int i = g * 32 + (int)lane;
+      const int gn = g + (int)planners;
+      nvshmemx_request rn;
+      if (gn < ngroups && gn * 32 + (int)lane < n) rn = load_request(reqs + gn * 32 + lane);  // prefetch
+      WorkItem w;
+      unsigned cnt = 0;
+      if (i < n) plan_one(c, r, i, chunk, bctl, w, cnt);
+      unsigned incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (unsigned)o) incl += v;
+      }
+      const unsigned tot = __shfl_sync(0xffffffffu, incl, 31);
+      unsigned long long base = 0;
+      if (lane == 31 && tot) {
+        base = atomicAdd(&ctl->total_chunks, (unsigned long long)tot);
+        if (base + tot > cap) set_status(bctl, NVSHMEMX_ERR_NOMEM, -1);
+      }
+      base = __shfl_sync(0xffffffffu, base, 31);
+      const unsigned long long first = base + incl - cnt;
+      for (unsigned k = 0; k < cnt && first + k < cap; ++k) {
+        WorkItem p = w;
+        const unsigned long long off = (unsigned long long)k * chunk;
+        p.dst += off;
+        p.src += off;
+        if (w.kind == kCopy) p.len = (unsigned)((w.len - off) < chunk ? (w.len - off) : chunk);
+        publish_item(items + first + k, p, gen);
+      }
+      r = rn;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence();
+      atomicAdd(&ctl->plan_done, 1u);
     }
   }
+  // ---- execution (every warp)
+  bool done = false, timed_out = false;
+  while (!done) {
+    unsigned long long bse = 0;
+    if (lane == 0) bse = atomicAdd(&ctl->cursor, (unsigned long long)grab);
+    bse = __shfl_sync(0xffffffffu, bse, 0);
+    for (unsigned long long k = bse; k < bse + (unsigned long long)grab; ++k) {
+      int st = 0;
+      if (lane == 0) st = wait_item(ctl, items, k, cap, gen, planners, ring.deadline);
+      st = __shfl_sync(0xffffffffu, st, 0);
+      if (st != 1) {
+        done = true;
+        timed_out = st == 3;
+        break;
+      }
+      ring.run(read_item(items + k), lane);
+    }
+  }
+  const bool ok = ring.drain(lane);
+  if ((timed_out || !ok) && lane == 0) {
+    if (atomicCAS(&ctl->status, 0, NVSHMEMX_ERR_TIMEOUT) == 0) ctl->bad_request = -2;
+  }
+}
+
+// Zeroes the control block of a streaming launch and moves its generation
+// on (one thread; a graph node in place of a memset).
+__global__ void stream_reset_kernel(StreamCtl *ctl) {
+  const unsigned g = ctl->gen + 1u;
+  ctl->total_chunks = 0;
+  ctl->cursor = 0;
+  ctl->status = 0;
+  ctl->bad_request = 0;
+  ctl->plan_done = 0;
+  ctl->gen = g == 0 ? 1u : g;
 }
 
 typedef void (*TmaFn)(const WorkItem *, BatchCtl *, unsigned long long, int, unsigned, unsigned, long long);
@@ -319,6 +562,39 @@ static TmaFn pick_tma(int stages) {
 
 static size_t tma_smem_bytes(const nvshmemx_batch_config &k) {
   return (size_t)(k.threads / 32) * (256 + (size_t)k.tma_stages * (size_t)k.tma_stage_bytes);
+}
+
+// Cooperative launch of the streaming kernel (every CTA must be resident:
+// executing warps wait for items that planning warps of other CTAs publish).
+static cudaError_t launch_stream(int stages, dim3 grid, dim3 block, size_t smem, cudaStream_t st, const Cfg &c,
+                                 const nvshmemx_request *src, int n, unsigned chunk, WorkItem *items,
+                                 unsigned long long cap, StreamCtl *ctl, int grab, unsigned SB, unsigned min_bulk,
+                                 int planners) {
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = grid;
+  lc.blockDim = block;
+  lc.dynamicSmemBytes = smem;
+  lc.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  lc.attrs = attr;
+  lc.numAttrs = 1;
+  switch (stages) {
+    case 2: return cudaLaunchKernelEx(&lc, batch_stream_kernel<2>, c, src, n, chunk, items, cap, ctl, grab, SB, min_bulk, planners);
+    case 3: return cudaLaunchKernelEx(&lc, batch_stream_kernel<3>, c, src, n, chunk, items, cap, ctl, grab, SB, min_bulk, planners);
+    case 4: return cudaLaunchKernelEx(&lc, batch_stream_kernel<4>, c, src, n, chunk, items, cap, ctl, grab, SB, min_bulk, planners);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+static const void *stream_fn(int stages) {
+  switch (stages) {
+    case 2: return (const void *)batch_stream_kernel<2>;
+    case 3: return (const void *)batch_stream_kernel<3>;
+    case 4: return (const void *)batch_stream_kernel<4>;
+    default: return nullptr;
+  }
 }
 
 typedef void (*ExecFn)(const WorkItem *, BatchCtl *, unsigned long long, int);
@@ -340,14 +616,19 @@ int check_batch_config(const nvshmemx_batch_config &c) {
                   (c.threads == 128 || c.threads == 256 || c.threads == 512 || c.threads == 1024) &&
                   c.ctas_per_sm >= 0 && c.ctas_per_sm <= 16 && c.grab >= 1 && c.grab <= 16;
   if (!ok) return NVSHMEMX_ERR_INVALID;
-  if (c.tma_stages == 0) return 0;
+  if (c.tma_stages == 0) return c.stream == 0 ? 0 : NVSHMEMX_ERR_INVALID;
   // TMA rings: at most 256 threads per CTA (8 warps, one ring each), stage
   // sizes in whole KiB, and the CTA's rings must fit in 227 KiB of shared
   // memory.
   const bool tma_ok = (c.tma_stages >= 2 && c.tma_stages <= 4) && c.threads <= 256 && c.tma_stage_bytes >= 1024 &&
                       c.tma_stage_bytes <= 32768 && (c.tma_stage_bytes % 1024) == 0 && c.tma_min_bytes >= 0 &&
                       tma_smem_bytes(c) <= 227u * 1024u;
-  return tma_ok ? 0 : NVSHMEMX_ERR_INVALID;
+  if (!tma_ok) return NVSHMEMX_ERR_INVALID;
+  // streaming needs the TMA rings and at least one executing-only warp
+  if (c.stream != 0 && (c.stream != 1 || c.stream_planners < 1 || c.stream_planners > 4 ||
+                        c.stream_planners >= c.threads / 32))
+    return NVSHMEMX_ERR_INVALID;
+  return 0;
 }
 
 }  // namespace nvshm
@@ -362,6 +643,7 @@ struct nvshmemx_batch {
   WorkItem *d_items = nullptr;
   BatchCtl *d_ctl = nullptr;
   nvshmemx_request *h_reqs = nullptr;  // pinned
+  const nvshmemx_request *h_reqs_dev = nullptr;  // h_reqs as the device sees it
   int *h_status = nullptr;             // pinned
   int n = 0;
   nvshmemx_batch_config cfg{};
@@ -369,6 +651,7 @@ struct nvshmemx_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   int graph_n = -1;
+  const nvshmemx_request *graph_src = nullptr;  // request array the graph reads
   nvshmemx_batch_config graph_cfg{};
   Cfg graph_arena{};
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr, ev_plan0 = nullptr, ev_exec0 = nullptr, ev_exec1 = nullptr;
@@ -383,12 +666,34 @@ static void drop_graph(nvshmemx_batch *b) {
   b->graph_n = -1;
 }
 
-// Enqueues memset + plan + exec on b->stream (used both for capture and for
-// the direct path).
-static int enqueue_batch(nvshmemx_batch *b, bool with_events) {
+// Enqueues memset + plan + exec (or, in stream mode, reset + the streaming
+// kernel) reading the requests at `src` on b->stream (used both for capture
+// and for the direct path).
+static int enqueue_batch(nvshmemx_batch *b, bool with_events, const nvshmemx_request *src) {
   const Runtime &r = rt();
   const Cfg c = r.cfg;
   const nvshmemx_batch_config &k = b->cfg;
+  if (k.stream) {
+    const void *sfn = stream_fn(k.tma_stages);
+    if (!sfn) return fail(NVSHMEMX_ERR_INVALID, "batch: no streaming kernel for %d stages", k.tma_stages);
+    (void)cudaGetLastError();
+    const size_t smem = tma_smem_bytes(k);
+    cudaFuncSetAttribute(sfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sfn, k.threads, smem);
+    if (per_sm < 1) return fail(NVSHMEMX_ERR_COOP, "batch: streaming kernel does not fit an SM");
+    const int ctas = k.ctas_per_sm > 0 && k.ctas_per_sm < per_sm ? k.ctas_per_sm : per_sm;
+    StreamCtl *sctl = reinterpret_cast<StreamCtl *>(b->d_ctl);
+    if (with_events) cudaEventRecord(b->ev_plan0, b->stream);
+    stream_reset_kernel<<<1, 1, 0, b->stream>>>(sctl);
+    if (with_events) cudaEventRecord(b->ev_exec0, b->stream);
+    cudaError_t e = launch_stream(k.tma_stages, dim3(r.sm_count * ctas), dim3(k.threads), smem, b->stream, c, src,
+                                  b->n, (unsigned)k.chunk_bytes, b->d_items, b->cap, sctl, k.grab,
+                                  (unsigned)k.tma_stage_bytes, (unsigned)k.tma_min_bytes, k.stream_planners);
+    if (with_events) cudaEventRecord(b->ev_exec1, b->stream);
+    if (e != cudaSuccess) return check_cuda(e, "batch streaming launch");
+    return check_cuda(cudaGetLastError(), "batch streaming launch");
+  }
   ExecFn fn = pick_exec(k.vec_bytes, k.unroll);
   TmaFn tfn = k.tma_stages ? pick_tma(k.tma_stages) : nullptr;
   if (!fn || (k.tma_stages && !tfn))
@@ -408,7 +713,7 @@ static int enqueue_batch(nvshmemx_batch *b, bool with_events) {
   cudaMemsetAsync(b->d_ctl, 0, sizeof(BatchCtl), b->stream);
   if (with_events) cudaEventRecord(b->ev_plan0, b->stream);
   if (b->n > 0)
-    batch_plan_kernel<<<(b->n + 255) / 256, 256, 0, b->stream>>>(c, b->d_reqs, b->n, (unsigned)k.chunk_bytes,
+    batch_plan_kernel<<<(b->n + 255) / 256, 256, 0, b->stream>>>(c, src, b->n, (unsigned)k.chunk_bytes,
                                                                  b->d_items, b->cap, b->d_ctl);
   if (with_events) cudaEventRecord(b->ev_exec0, b->stream);
   if (tfn)
@@ -421,16 +726,16 @@ static int enqueue_batch(nvshmemx_batch *b, bool with_events) {
   return check_cuda(cudaGetLastError(), "batch launch");
 }
 
-static int ensure_graph(nvshmemx_batch *b) {
+static int ensure_graph(nvshmemx_batch *b, const nvshmemx_request *src) {
   const Cfg &c = rt().cfg;
-  if (b->gexec && b->graph_n == b->n && memcmp(&b->graph_cfg, &b->cfg, sizeof b->cfg) == 0 &&
+  if (b->gexec && b->graph_n == b->n && b->graph_src == src && memcmp(&b->graph_cfg, &b->cfg, sizeof b->cfg) == 0 &&
       memcmp(&b->graph_arena, &c, sizeof c) == 0)
     return 0;
   drop_graph(b);
   int rc;
   if ((rc = check_cuda(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture")))
     return rc;
-  int erc = enqueue_batch(b, false);
+  int erc = enqueue_batch(b, false, src);
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaStreamEndCapture(b->stream, &g);
   if (erc) {
@@ -444,6 +749,7 @@ static int ensure_graph(nvshmemx_batch *b) {
     return rc;
   }
   b->graph_n = b->n;
+  b->graph_src = src;
   b->graph_cfg = b->cfg;
   b->graph_arena = c;
   return 0;
@@ -464,6 +770,8 @@ void nvshmemx_batch_default_config(nvshmemx_batch_config *c) {
   c->tma_stages = 3;
   c->tma_stage_bytes = 8192;
   c->tma_min_bytes = 512;
+  c->stream = 0;
+  c->stream_planners = 2;
 }
 
 int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes, int min_chunk_bytes,
@@ -480,7 +788,7 @@ int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes
   int rc = 0;
   if ((rc = check_cuda(cudaMalloc(&b->d_reqs, (size_t)max_requests * sizeof(nvshmemx_request)), "cudaMalloc(reqs)")) ||
       (rc = check_cuda(cudaMalloc(&b->d_items, (size_t)b->cap * sizeof(WorkItem)), "cudaMalloc(items)")) ||
-      (rc = check_cuda(cudaMalloc(&b->d_ctl, sizeof(BatchCtl)), "cudaMalloc(ctl)")) ||
+      (rc = check_cuda(cudaMalloc(&b->d_ctl, 128), "cudaMalloc(ctl)")) ||
       (rc = check_cuda(cudaMallocHost(&b->h_reqs, (size_t)max_requests * sizeof(nvshmemx_request)),
                        "cudaMallocHost(reqs)")) ||
       (rc = check_cuda(cudaMallocHost(&b->h_status, 64), "cudaMallocHost(status)")) ||
@@ -493,7 +801,16 @@ int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes
   cudaEventCreate(&b->ev_plan0);
   cudaEventCreate(&b->ev_exec0);
   cudaEventCreate(&b->ev_exec1);
-  cudaMemset(b->d_ctl, 0, sizeof(BatchCtl));
+  // control block (BatchCtl or StreamCtl) and every work item's generation
+  // tag start at zero; streaming generations start at 1
+  cudaMemset(b->d_ctl, 0, 128);
+  cudaMemset(b->d_items, 0, (size_t)b->cap * sizeof(WorkItem));
+  void *dev_alias = nullptr;
+  if ((rc = check_cuda(cudaHostGetDevicePointer(&dev_alias, b->h_reqs, 0), "cudaHostGetDevicePointer"))) {
+    nvshmemx_batch_destroy(b);
+    return rc;
+  }
+  b->h_reqs_dev = static_cast<const nvshmemx_request *>(dev_alias);
   *out = b;
   return 0;
 }
@@ -545,7 +862,7 @@ int nvshmemx_batch_upload(nvshmemx_batch *b, const nvshmemx_request *reqs, int n
 int nvshmemx_batch_execute(nvshmemx_batch *b, int reps, float *out_ms) {
   if (!b || reps < 1) return fail(NVSHMEMX_ERR_INVALID, "batch_execute: bad arguments");
   int rc;
-  if ((rc = ensure_graph(b))) return rc;
+  if ((rc = ensure_graph(b, b->d_reqs))) return rc;
   cudaEventRecord(b->ev_start, b->stream);
   for (int i = 0; i < reps; ++i)
     if ((rc = check_cuda(cudaGraphLaunch(b->gexec, b->stream), "cudaGraphLaunch"))) return rc;
@@ -564,9 +881,13 @@ int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n
   if (!b || n < 0 || n > b->max_n) return fail(NVSHMEMX_ERR_INVALID, "batch_submit: n outside [0, max]");
   int rc;
   b->n = n;
-  if ((rc = ensure_graph(b))) return rc;
+  // In stream mode the batch's own pinned buffer is read by the kernel over
+  // the host link while execution is already running; any other source is
+  // first copied to device memory.
+  const bool zero_copy = b->cfg.stream && reqs == b->h_reqs;
+  if ((rc = ensure_graph(b, zero_copy ? b->h_reqs_dev : b->d_reqs))) return rc;
   cudaEventRecord(b->ev_start, b->stream);
-  if (n &&
+  if (n && !zero_copy &&
       (rc = check_cuda(cudaMemcpyAsync(b->d_reqs, reqs, (size_t)n * sizeof(nvshmemx_request), cudaMemcpyHostToDevice,
                                        b->stream),
                        "cudaMemcpyAsync(requests)")))
@@ -612,7 +933,7 @@ int nvshmemx_batch_execute_direct(nvshmemx_batch *b, int reps, float *out_ms, fl
   float total = 0, exec = 0;
   for (int i = 0; i < reps; ++i) {
     cudaEventRecord(b->ev_start, b->stream);
-    if ((rc = enqueue_batch(b, true))) return rc;
+    if ((rc = enqueue_batch(b, true, b->d_reqs))) return rc;
     cudaEventRecord(b->ev_stop, b->stream);
     if ((rc = check_cuda(cudaStreamSynchronize(b->stream), "batch_execute_direct"))) return rc;
     float t = 0, e = 0;

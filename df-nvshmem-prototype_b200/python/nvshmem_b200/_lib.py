@@ -46,7 +46,8 @@ assert TRACE_DTYPE.itemsize == 48
 class BatchConfig(ctypes.Structure):
     _fields_ = [("vec_bytes", c_int), ("chunk_bytes", c_int), ("unroll", c_int),
                 ("threads", c_int), ("ctas_per_sm", c_int), ("grab", c_int),
-                ("tma_stages", c_int), ("tma_stage_bytes", c_int), ("tma_min_bytes", c_int)]
+                ("tma_stages", c_int), ("tma_stage_bytes", c_int), ("tma_min_bytes", c_int),
+                ("stream", c_int), ("stream_planners", c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

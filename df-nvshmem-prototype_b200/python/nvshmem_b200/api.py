@@ -196,6 +196,7 @@ class Batch:
         if isinstance(cfg, dict):
             c = default_batch_config()
             c.tma_stages = 0
+            c.stream = 0
             for k, v in cfg.items():
                 setattr(c, k, int(v))
             cfg = c

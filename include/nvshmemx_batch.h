@@ -45,6 +45,14 @@ typedef struct nvshmemx_batch_config {
                        many shared-memory stages with cp.async.bulk          */
   int tma_stage_bytes; /* bytes per stage: multiple of 1024, 1 KiB..32 KiB    */
   int tma_min_bytes;   /* chunks shorter than this use the register copy    */
+  int stream;          /* 1: plan and execute in one persistent cooperative
+                          launch, planning warps feeding executing warps
+                          (needs tma_stages > 0); the end-to-end call then
+                          reads the requests straight from the pinned host
+                          buffer.  An invalid request is skipped on its own
+                          and reported, the others still run.  0: a graph of
+                          plan then exec; an invalid request stops the batch */
+  int stream_planners; /* planning warps per CTA in stream mode: 1..4        */
 } nvshmemx_batch_config;
 
 /* Defaults for B200: the best configuration the autotuner measured on the

@@ -25,7 +25,15 @@ CONFIGS = [
          tma_stages=4, tma_stage_bytes=4096, tma_min_bytes=2048),
     dict(vec_bytes=16, chunk_bytes=1024, unroll=4, threads=256, ctas_per_sm=1, grab=1,
          tma_stages=2, tma_stage_bytes=1024, tma_min_bytes=16),
+    # streaming: planning warps feed executing warps inside one launch
+    dict(vec_bytes=16, chunk_bytes=16384, unroll=4, threads=256, ctas_per_sm=0, grab=2,
+         tma_stages=3, tma_stage_bytes=8192, tma_min_bytes=512, stream=1, stream_planners=2),
+    dict(vec_bytes=16, chunk_bytes=1024, unroll=4, threads=128, ctas_per_sm=1, grab=1,
+         tma_stages=2, tma_stage_bytes=4096, tma_min_bytes=0, stream=1, stream_planners=1),
 ]
+
+STREAM = dict(vec_bytes=16, chunk_bytes=16384, unroll=4, threads=256, ctas_per_sm=0, grab=2,
+              tma_stages=3, tma_stage_bytes=8192, tma_min_bytes=512, stream=1, stream_planners=2)
 
 
 def setup(shmem_factory, npes, heap, seed=7):
@@ -100,6 +108,54 @@ def test_submit_end_to_end(shmem_factory):
     assert first_diff(heap_images(sh, npes, heap), om.heap) is None
 
 
+def test_stream_submit_reads_pinned_host_buffer(shmem_factory):
+    """End-to-end in stream mode: the kernel reads the requests from the
+    batch's pinned host buffer while it executes; two different batches in a
+    row through the same buffer (generation tags keep them apart)."""
+    npes, heap = 8, 8 << 20
+    sh, om = setup(shmem_factory, npes, heap)
+    with sh.batch(4000, 64 << 20, 4096) as b:
+        b.set_config(STREAM)
+        buf = b.host_buffer()
+        for seed in (41, 42):
+            reqs = c4_batch(seed=seed, n=3000, npes=npes, heap=heap, hi=128 << 10)
+            buf[:len(reqs)] = reqs
+            st, ms = b.submit(buf, len(reqs))
+            assert st == 0 and ms > 0
+            om.apply_requests(reqs)
+            assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+        # device-resident execution of the same object (graph of the stream kernel)
+        reqs = c4_batch(seed=43, n=2500, npes=npes, heap=heap, hi=128 << 10)
+        b.upload(reqs)
+        b.execute(2)
+        om.apply_requests(reqs)
+        assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+        # switching between graph and stream modes on one object stays exact
+        b.set_config(dict(STREAM, stream=0))
+        b.execute(1)
+        b.set_config(STREAM)
+        b.execute(1)
+        assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+    assert sh.status() == 0
+
+
+def test_stream_skips_invalid_requests_individually(shmem_factory):
+    npes, heap = 4, 1 << 20
+    sh, om = setup(shmem_factory, npes, heap)
+    good = c4_batch(seed=44, n=600, npes=npes, heap=heap, hi=8 << 10)
+    bad = requests([dict(src_off=0, dst_off=heap - 16, bytes=64, src_pe=0, dst_pe=1, op=REQ_PUT, dtype=0),
+                    dict(src_off=0, dst_off=heap // 2, bytes=64, src_pe=0, dst_pe=9, op=REQ_PUT, dtype=0)])
+    reqs = np.concatenate([good[:300], bad, good[300:]])
+    with sh.batch(len(reqs), int(good["bytes"].sum()) + 128, 256) as b:
+        b.set_config(dict(STREAM, chunk_bytes=4096))
+        b.upload(reqs)
+        with pytest.raises(Exception):
+            b.execute(1)  # reports the first bad request ...
+    sh.status()
+    om.apply_requests(good)  # ... but the valid ones ran
+    assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+
+
 def test_bad_request_rejected_not_executed(shmem_factory):
     npes, heap = 4, 1 << 20
     sh, om = setup(shmem_factory, npes, heap)
@@ -121,19 +177,27 @@ def test_empty_batch(shmem_factory):
     assert sh.status() == 0
 
 
-@pytest.mark.parametrize("tma", [0, 3])
-def test_c4_full_size_checksums(shmem_factory, tma):
+@pytest.mark.parametrize("mode", ["register", "tma", "stream"])
+def test_c4_full_size_checksums(shmem_factory, mode):
     """The benchmark's batch: 64 PEs x 64 MiB, 100,000 requests."""
     npes, heap = 64, 64 << 20
     reqs = c4_batch(seed=4, n=100_000, npes=npes, heap=heap)
     assert check_disjoint(reqs)
     sh, om = setup(shmem_factory, npes, heap, seed=44)
     with sh.batch(len(reqs), int(reqs["bytes"].sum()), 4096) as b:
-        if tma:
+        if mode == "register":
+            b.set_config(CONFIGS[0])
+        elif mode == "tma":
             b.set_config(dict(vec_bytes=16, chunk_bytes=16384, unroll=4, threads=256, ctas_per_sm=0, grab=2,
-                              tma_stages=tma, tma_stage_bytes=8192, tma_min_bytes=1024))
+                              tma_stages=3, tma_stage_bytes=8192, tma_min_bytes=1024))
+        else:
+            b.set_config(STREAM)
         b.upload(reqs)
         b.execute(3)
+        if mode == "stream":
+            buf = b.host_buffer()
+            buf[:len(reqs)] = reqs
+            assert b.submit(buf, len(reqs))[0] == 0
     assert sh.status() == 0
     om.apply_requests(reqs)
     for pe in range(npes):
