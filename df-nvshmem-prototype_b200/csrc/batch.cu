@@ -402,14 +402,17 @@ __device__ __forceinline__ void plan_one(const Cfg &c, const nvshmemx_request &r
   }
 }
 
-__device__ __forceinline__ void publish_item(WorkItem *p, const WorkItem &w, unsigned gen) {
+// The item's payload (its first 28 bytes), written with plain stores; the
+// generation tag in the last word is stored separately, after a fence.
+__device__ __forceinline__ void write_item_body(WorkItem *p, const WorkItem &w) {
   uint4 a = make_uint4((unsigned)w.dst, (unsigned)(w.dst >> 32), (unsigned)w.src, (unsigned)(w.src >> 32));
   *reinterpret_cast<uint4 *>(p) = a;
   uint2 b = make_uint2(w.len, w.kind);
   *reinterpret_cast<uint2 *>(reinterpret_cast<char *>(p) + 16) = b;
   *reinterpret_cast<int *>(reinterpret_cast<char *>(p) + 24) = w.value;
-  st_release_b32(reinterpret_cast<char *>(p) + 28, gen);
 }
+
+__device__ __forceinline__ void *item_tag(WorkItem *p) { return reinterpret_cast<char *>(p) + 28; }
 
 __device__ __forceinline__ WorkItem read_item(const WorkItem *p) {
   const uint4 a = __ldcg(reinterpret_cast<const uint4 *>(p));
@@ -434,20 +437,28 @@ __device__ __forceinline__ nvshmemx_request load_request(const nvshmemx_request 
 }
 
 // 1: item k is ready; 2: there is no item k (all planning done and k is past
-// the end, or past the table); 3: the deadline passed.
+// the end, or past the table); 3: the deadline passed.  `final_total` is the
+// calling lane's cache of the chunk count: ~0 until it has seen every planner
+// finish (an acquire of plan_done, which orders every published item before
+// this lane's later reads), after which no item needs a check at all.
 __device__ __forceinline__ int wait_item(StreamCtl *ctl, const WorkItem *items, unsigned long long k,
                                          unsigned long long cap, unsigned gen, unsigned planners,
-                                         unsigned long long deadline) {
+                                         unsigned long long deadline, unsigned long long &final_total) {
   if (k >= cap) return 2;
+  if (final_total != ~0ull) return k < final_total ? 1 : 2;
   const int *tag = reinterpret_cast<const int *>(reinterpret_cast<const char *>(items + k) + 28);
   unsigned ns = 0;
   for (unsigned spins = 0;; ++spins) {
-    if (k < ld_acquire_u64(&ctl->total_chunks)) {
-      if ((unsigned)ld_acquire(tag) == gen) return 1;
-    } else if ((unsigned)ld_acquire(reinterpret_cast<const int *>(&ctl->plan_done)) == planners) {
-      if (k >= ld_acquire_u64(&ctl->total_chunks)) return 2;
-      continue;
+    // both loads in flight at once: a relaxed read of plan_done that sees
+    // every planner done is followed by a fence (the acquire pattern)
+    const unsigned pd = ld_relaxed_b32(&ctl->plan_done);
+    const unsigned tg = (unsigned)ld_acquire(tag);
+    if (pd == planners) {
+      asm volatile("fence.acq_rel.gpu;" ::: "memory");
+      final_total = ld_acquire_u64(&ctl->total_chunks);
+      return k < final_total ? 1 : 2;
     }
+    if (tg == gen) return 1;
     if (spins > 8) {
       ns = ns == 0 ? 32 : (ns >= 512 ? 512 : ns * 2);
       __nanosleep(ns);
@@ -497,14 +508,19 @@ __global__ void __launch_bounds__(256) batch_stream_kernel(Cfg c, const nvshmemx
       }
       base = __shfl_sync(0xffffffffu, base, 31);
       const unsigned long long first = base + incl - cnt;
-      for (unsigned k = 0; k < cnt && first + k < cap; ++k) {
+      const unsigned last = first + cnt <= cap ? cnt : (first < cap ? (unsigned)(cap - first) : 0u);
+      for (unsigned k = 0; k < last; ++k) {
         WorkItem p = w;
         const unsigned long long off = (unsigned long long)k * chunk;
         p.dst += off;
         p.src += off;
         if (w.kind == kCopy) p.len = (unsigned)((w.len - off) < chunk ? (w.len - off) : chunk);
-        publish_item(items + first + k, p, gen);
+        write_item_body(items + first + k, p);
       }
+      // one fence per group orders every payload before its tag (a release
+      // pattern: fence, then strong stores); consumers acquire the tag
+      __threadfence();
+      for (unsigned k = 0; k < last; ++k) st_relaxed_b32(item_tag(items + first + k), gen);
       r = rn;
     }
     __syncwarp();
@@ -513,26 +529,26 @@ __global__ void __launch_bounds__(256) batch_stream_kernel(Cfg c, const nvshmemx
       atomicAdd(&ctl->plan_done, 1u);
     }
   }
-  // ---- execution (every warp)
-  bool done = false, timed_out = false;
-  while (!done) {
-    unsigned long long bse = 0;
-    if (lane == 0) bse = atomicAdd(&ctl->cursor, (unsigned long long)grab);
-    bse = __shfl_sync(0xffffffffu, bse, 0);
+  // ---- execution (every warp); the next claim is in flight while the
+  // current one runs, as in the graph path
+  unsigned long long final_total = ~0ull;
+  int st = 1;
+  unsigned long long bse = 0;
+  if (lane == 0) bse = atomicAdd(&ctl->cursor, (unsigned long long)grab);
+  bse = __shfl_sync(0xffffffffu, bse, 0);
+  while (st == 1) {
+    unsigned long long nxt = 0;
+    if (lane == 0) nxt = atomicAdd(&ctl->cursor, (unsigned long long)grab);
     for (unsigned long long k = bse; k < bse + (unsigned long long)grab; ++k) {
-      int st = 0;
-      if (lane == 0) st = wait_item(ctl, items, k, cap, gen, planners, ring.deadline);
+      if (lane == 0) st = wait_item(ctl, items, k, cap, gen, planners, ring.deadline, final_total);
       st = __shfl_sync(0xffffffffu, st, 0);
-      if (st != 1) {
-        done = true;
-        timed_out = st == 3;
-        break;
-      }
+      if (st != 1) break;
       ring.run(read_item(items + k), lane);
     }
+    bse = __shfl_sync(0xffffffffu, nxt, 0);
   }
   const bool ok = ring.drain(lane);
-  if ((timed_out || !ok) && lane == 0) {
+  if ((st == 3 || !ok) && lane == 0) {
     if (atomicCAS(&ctl->status, 0, NVSHMEMX_ERR_TIMEOUT) == 0) ctl->bad_request = -2;
   }
 }

@@ -328,40 +328,32 @@ __device__ __forceinline__ bool bulk_copy_1t(const BulkRing &ring, char *dst, co
 // 16-aligned body while the other threads copy the unaligned head and tail.
 // Falls back to the generic copy when dst/src alignments differ mod 16 or the
 // ring has no room.  Every thread of the block must call it.
-// The body is split into one contiguous 16-byte-aligned range per warp and
-// every warp's lane 0 drives its own 3-stage ring in its share of `smem`, so
-// a CTA has as many TMA issuers as warps (one issuer per CTA leaves the copy
-// short of bytes in flight); lanes 1..31 of the first and last warps copy the
-// unaligned head and tail.
+// One issuer per CTA streams the body as one sequential range: measured on
+// B200 this keeps DRAM accesses more local than splitting the range across
+// per-warp rings (which lost 6-7% on 16-256 MiB all-to-all rounds).
 __device__ __forceinline__ void bulk_copy_block(const Cfg &c, char *dst, const char *src,
                                                 unsigned long long bytes, void *smem,
                                                 unsigned smem_bytes) {
   const unsigned r = block_rank(), n = block_size();
-  const unsigned nw = n / 32, warp = r / 32, lane = r % 32;
-  const unsigned per_warp = nw ? (smem_bytes / nw) & ~127u : 0;
-  BulkRing ring = make_ring(reinterpret_cast<char *>(smem) + (size_t)warp * per_warp, per_warp, 3);
+  BulkRing ring = make_ring(smem, smem_bytes, 4);
   if ((((uintptr_t)dst ^ (uintptr_t)src) & 15) != 0 || ring.stage_bytes < 1024 || bytes < 4096 ||
-      n < 64 || (n & 31) != 0) {
+      n < 64) {
     copy_coop<16, 4>(dst, src, bytes, r, n);
     __syncthreads();
     return;
   }
-  const unsigned long long head = (16 - ((uintptr_t)dst & 15)) & 15;
-  const unsigned long long body = (bytes - head) & ~15ull;
-  const unsigned long long tail = bytes - head - body;
-  const unsigned long long share = ((body + nw - 1) / nw + 15) & ~15ull;
-  const unsigned long long wb = (unsigned long long)warp * share;
-  const unsigned long long we = wb + share < body ? wb + share : body;
-  if (lane == 0) {
-    if (wb < we) {
-      const unsigned long long deadline = gtimer() + (unsigned long long)c.wait_timeout_ns;
-      if (!bulk_copy_1t(ring, dst + head + wb, src + head + wb, we - wb, deadline))
-        record_error(c, NVSHMEMX_ERR_TIMEOUT, -2);
-    }
-  } else if (warp == 0) {
-    for (unsigned long long i = lane - 1; i < head; i += 31) dst[i] = src[i];
-  } else if (warp == nw - 1) {
-    for (unsigned long long i = lane - 1; i < tail; i += 31) dst[head + body + i] = src[head + body + i];
+  unsigned long long head = (16 - ((uintptr_t)dst & 15)) & 15;
+  unsigned long long body = (bytes - head) & ~15ull;
+  unsigned long long tail = bytes - head - body;
+  if (r == 0) {
+    unsigned long long deadline = gtimer() + (unsigned long long)c.wait_timeout_ns;
+    if (!bulk_copy_1t(ring, dst + head, src + head, body, deadline))
+      record_error(c, NVSHMEMX_ERR_TIMEOUT, -2);
+  } else if (r >= 32) {
+    // warps 1.. handle head and tail bytes
+    unsigned rr = r - 32, nn = n - 32;
+    for (unsigned long long i = rr; i < head; i += nn) dst[i] = src[i];
+    for (unsigned long long i = rr; i < tail; i += nn) dst[head + body + i] = src[head + body + i];
   }
   __syncthreads();
 }

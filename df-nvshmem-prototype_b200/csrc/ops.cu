@@ -429,9 +429,9 @@ static int last_launch(const char *what) {
   return check_cuda(cudaGetLastError(), what);
 }
 
-// Shared memory for the CTA-wide TMA copies: one 3 x 8 KiB ring (plus 128
-// bytes of mbarriers) for each of the 8 warps of a 256-thread CTA.
-static const unsigned kBulkSmem = 8 * (128 + 3 * 8192);
+// Shared memory for the CTA-wide TMA copies: a 4 x 16 KiB ring plus 128
+// bytes of mbarriers (three CTAs fit an SM).
+static const unsigned kBulkSmem = 4 * 16384 + 128;
 
 namespace nvshm {
 int launch_exec_requests(int mode, const nvshmemx_request *dr, int n, cudaStream_t s) {

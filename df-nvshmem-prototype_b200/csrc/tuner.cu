@@ -84,17 +84,18 @@ int nvshmemx_tune_candidates(nvshmemx_batch_config *out, int max, int min_chunk_
             c.tma_min_bytes = mb;
             push(c);
           }
-  // streaming (plan and execute in one launch): stages x planning warps
-  for (int s : {2, 3})
+  // streaming (plan and execute in one launch): ring shape x planning warps
+  struct Ring { int threads, stages, stage_bytes; };
+  for (Ring g : {Ring{128, 4, 4096}, Ring{256, 3, 8192}, Ring{256, 4, 4096}})
     for (int pl : {1, 2}) {
       c.vec_bytes = 16;
       c.unroll = 4;
       c.chunk_bytes = 16384;
-      c.threads = 256;
+      c.threads = g.threads;
       c.ctas_per_sm = 0;
       c.grab = 2;
-      c.tma_stages = s;
-      c.tma_stage_bytes = 8192;
+      c.tma_stages = g.stages;
+      c.tma_stage_bytes = g.stage_bytes;
       c.tma_min_bytes = 512;
       c.stream = 1;
       c.stream_planners = pl;
