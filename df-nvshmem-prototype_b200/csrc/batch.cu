@@ -12,6 +12,8 @@
 //            chunk with VB-byte accesses, U in flight per lane.
 // Every chunk is a contiguous copy, so the exec kernel is pure streaming:
 // its roofline is HBM copy bandwidth (2 bytes moved per payload byte).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <string.h>
@@ -34,11 +36,11 @@ struct WorkItem {          // 32 bytes
 enum { kCopy = 0, kSignal = 1, kStore = 2 };
 
 struct BatchCtl {  // 32 bytes, zeroed before every execution
-  unsigned long long total_chunks;
+  unsigned long long total_chunks;  // chunks of this piece of the batch
   unsigned long long cursor;
   int status;
   int bad_request;
-  unsigned long long pad;
+  unsigned long long item_base;     // index of the piece's first work item
 };
 
 __device__ __forceinline__ void set_status(BatchCtl *ctl, int code, int req) {
@@ -46,11 +48,18 @@ __device__ __forceinline__ void set_status(BatchCtl *ctl, int code, int req) {
 }
 
 // ------------------------------------------------------------------- plan
+// A batch is planned as one piece, or (pipelined submit) as consecutive
+// pieces: piece p appends its items after those of piece p-1 (`prev`, planned
+// earlier on the same stream) and reports errors, with request indices
+// offset by `req_base`, in the first piece's control block `sctl`.
 __global__ void __launch_bounds__(256) batch_plan_kernel(Cfg c, const nvshmemx_request *__restrict__ reqs, int n,
                                                          unsigned chunk, WorkItem *__restrict__ items,
-                                                         unsigned long long cap, BatchCtl *ctl) {
+                                                         unsigned long long cap, BatchCtl *ctl, BatchCtl *sctl,
+                                                         const BatchCtl *prev, int req_base) {
   __shared__ unsigned warp_sums[8];
   __shared__ unsigned long long block_base;
+  const unsigned long long ibase = prev ? prev->item_base + prev->total_chunks : 0ull;
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->item_base = ibase;
   const int i = blockIdx.x * 256 + threadIdx.x;
   const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   unsigned cnt = 0;
@@ -72,7 +81,7 @@ __global__ void __launch_bounds__(256) batch_plan_kernel(Cfg c, const nvshmemx_r
       case NVSHMEMX_REQ_G: {
         const unsigned long long bytes = r.op == NVSHMEMX_REQ_G ? width : r.bytes;
         if (!pe_ok || r.src_off + bytes > c.slice_bytes || r.dst_off + bytes > c.slice_bytes) {
-          set_status(ctl, NVSHMEMX_ERR_BOUNDS, i);
+          set_status(sctl, NVSHMEMX_ERR_BOUNDS, req_base + i);
           break;
         }
         w.dst = dst;
@@ -85,7 +94,7 @@ __global__ void __launch_bounds__(256) batch_plan_kernel(Cfg c, const nvshmemx_r
       case NVSHMEMX_REQ_P: {
         const unsigned bytes = r.op == NVSHMEMX_REQ_SIGNAL ? 4u : width;
         if (!pe_ok || r.dst_off + bytes > c.slice_bytes || (r.dst_off & (bytes - 1))) {
-          set_status(ctl, NVSHMEMX_ERR_BOUNDS, i);
+          set_status(sctl, NVSHMEMX_ERR_BOUNDS, req_base + i);
           break;
         }
         w.dst = dst;
@@ -97,7 +106,7 @@ __global__ void __launch_bounds__(256) batch_plan_kernel(Cfg c, const nvshmemx_r
         break;
       }
       default:
-        set_status(ctl, NVSHMEMX_ERR_INVALID, i);
+        set_status(sctl, NVSHMEMX_ERR_INVALID, req_base + i);
     }
   }
   // CTA-wide exclusive scan of cnt
@@ -117,11 +126,11 @@ __global__ void __launch_bounds__(256) batch_plan_kernel(Cfg c, const nvshmemx_r
       acc += s;
     }
     block_base = acc ? atomicAdd(&ctl->total_chunks, (unsigned long long)acc) : 0ull;
-    if (acc && block_base + acc > cap) set_status(ctl, NVSHMEMX_ERR_NOMEM, -1);
+    if (acc && ibase + block_base + acc > cap) set_status(sctl, NVSHMEMX_ERR_NOMEM, -1);
   }
   __syncthreads();
   if (cnt == 0) return;
-  const unsigned long long first = block_base + warp_sums[warp] + (incl - cnt);
+  const unsigned long long first = ibase + block_base + warp_sums[warp] + (incl - cnt);
   if (first + cnt > cap) return;
   if (cnt == 1) {
     items[first] = w;
@@ -171,11 +180,13 @@ __device__ __forceinline__ void run_item(const WorkItem &w, unsigned lane) {
 
 template <int VB, int U>
 __global__ void __launch_bounds__(1024) batch_exec_kernel(const WorkItem *__restrict__ items, BatchCtl *ctl,
-                                                          unsigned long long cap, int grab) {
+                                                          const BatchCtl *sctl, unsigned long long cap, int grab) {
   const unsigned lane = threadIdx.x & 31u;
-  if (*(volatile int *)&ctl->status != 0) return;
+  if (*(volatile const int *)&sctl->status != 0) return;
   unsigned long long C = *(volatile unsigned long long *)&ctl->total_chunks;
-  if (C > cap) return;
+  const unsigned long long ib = *(volatile unsigned long long *)&ctl->item_base;
+  if (ib + C > cap) return;
+  items += ib;
   unsigned long long base = 0;
   if (lane == 0) base = atomicAdd(&ctl->cursor, (unsigned long long)grab);
   base = __shfl_sync(0xffffffffu, base, 0);
@@ -304,13 +315,15 @@ struct WarpTma {
 
 template <int S>
 __global__ void __launch_bounds__(256) batch_exec_tma_kernel(const WorkItem *__restrict__ items, BatchCtl *ctl,
-                                                              unsigned long long cap, int grab, unsigned SB,
-                                                              unsigned min_bulk, long long timeout_ns) {
+                                                              BatchCtl *sctl, unsigned long long cap, int grab,
+                                                              unsigned SB, unsigned min_bulk, long long timeout_ns) {
   extern __shared__ __align__(128) char smem[];
   const unsigned lane = threadIdx.x & 31u;
-  if (*(volatile int *)&ctl->status != 0) return;
+  if (*(volatile int *)&sctl->status != 0) return;
   const unsigned long long C = *(volatile unsigned long long *)&ctl->total_chunks;
-  if (C > cap) return;
+  const unsigned long long ib = *(volatile unsigned long long *)&ctl->item_base;
+  if (ib + C > cap) return;
+  items += ib;
   WarpTma<S> ring;
   ring.init(smem, SB, min_bulk, timeout_ns, lane);
   unsigned long long bse = 0;
@@ -324,7 +337,7 @@ __global__ void __launch_bounds__(256) batch_exec_tma_kernel(const WorkItem *__r
     bse = __shfl_sync(0xffffffffu, nxt, 0);
   }
   if (!ring.drain(lane) && lane == 0) {
-    if (atomicCAS(&ctl->status, 0, NVSHMEMX_ERR_TIMEOUT) == 0) ctl->bad_request = -2;
+    if (atomicCAS(&sctl->status, 0, NVSHMEMX_ERR_TIMEOUT) == 0) sctl->bad_request = -2;
   }
 }
 
@@ -352,8 +365,12 @@ struct StreamCtl {                 // the first 32 bytes match BatchCtl
   unsigned int gen;                // generation of the current launch; outside
                                    // the 32 bytes the graph path zeroes, so it
                                    // only ever grows
-  unsigned long long pad[3];
+  unsigned int reqs_ready;         // staged submit: requests resident so far,
+                                   // written by the copy stream after each piece
+  unsigned int plan_cursor;        // next group of 32 requests to plan
+  unsigned long long pad[2];
 };
+static_assert(sizeof(StreamCtl) == 64, "StreamCtl is one 64-byte block");
 
 __device__ __forceinline__ void plan_one(const Cfg &c, const nvshmemx_request &r, int i, unsigned chunk,
                                          BatchCtl *ctl, WorkItem &w, unsigned &cnt) {
@@ -471,7 +488,8 @@ template <int S>
 __global__ void __launch_bounds__(256) batch_stream_kernel(Cfg c, const nvshmemx_request *reqs, int n,
                                                            unsigned chunk, WorkItem *__restrict__ items,
                                                            unsigned long long cap, StreamCtl *ctl, int grab,
-                                                           unsigned SB, unsigned min_bulk, int planners_per_cta) {
+                                                           unsigned SB, unsigned min_bulk, int planners_per_cta,
+                                                           const unsigned *ready, int resident0) {
   extern __shared__ __align__(128) char smem[];
   const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   BatchCtl *bctl = reinterpret_cast<BatchCtl *>(ctl);
@@ -481,16 +499,58 @@ __global__ void __launch_bounds__(256) batch_stream_kernel(Cfg c, const nvshmemx
   ring.init(smem, SB, min_bulk, c.wait_timeout_ns, lane);
   // ---- planning (the first planners_per_cta warps of each CTA)
   if (warp < (unsigned)planners_per_cta) {
-    const unsigned me = blockIdx.x * (unsigned)planners_per_cta + warp;
     const int ngroups = (n + 31) / 32;
-    int g = (int)me;
+    // Requests known to be resident: all of them, or (staged submit) the
+    // first `resident0` plus the count the copy stream has published in
+    // *ready since, refreshed on demand.
+    int rdy = ready ? resident0 : n;
+    auto refresh = [&](int upto) -> bool {
+      int v = 0;
+      if (lane == 0) {
+        unsigned ns = 0;
+        for (unsigned spins = 0;; ++spins) {
+          v = ld_acquire(reinterpret_cast<const int *>(ready));
+          if (v >= upto) break;
+          ns = ns == 0 ? 64 : (ns >= 1024 ? 1024 : ns * 2);
+          __nanosleep(ns);
+          if ((spins & 15) == 15 && gtimer() > ring.deadline) {
+            v = -1;
+            break;
+          }
+        }
+      }
+      v = __shfl_sync(0xffffffffu, v, 0);
+      if (v < 0) return false;
+      rdy = v > rdy ? v : rdy;
+      return true;
+    };
+    // groups are claimed in request order, so planning follows the pieces
+    // as they land and items are published roughly in request order
+    auto claim = [&]() -> int {
+      int v = 0;
+      if (lane == 0) v = (int)atomicAdd(&ctl->plan_cursor, 1u);
+      return __shfl_sync(0xffffffffu, v, 0);
+    };
+    int g = claim();
     nvshmemx_request r;
-    if (g < ngroups && g * 32 + (int)lane < n) r = load_request(reqs + g * 32 + lane);
-    for (; g < ngroups; g += (int)planners) {
+    bool ok_ready = true;
+    if (g < ngroups) {
+      const int hi = g * 32 + 32 < n ? g * 32 + 32 : n;
+      ok_ready = hi <= rdy || refresh(hi);
+      if (ok_ready && g * 32 + (int)lane < n) r = load_request(reqs + g * 32 + lane);
+    }
+    for (; g < ngroups && ok_ready;) {
       const int i = g * 32 + (int)lane;
-      const int gn = g + (int)planners;
+      // claim the next group and fetch it while this one is planned, if it
+      // is resident already
+      const int gn = claim();
       nvshmemx_request rn;
-      if (gn < ngroups && gn * 32 + (int)lane < n) rn = load_request(reqs + gn * 32 + lane);  // prefetch
+      bool have = false;
+      const int hn = gn * 32 + 32 < n ? gn * 32 + 32 : n;
+      if (gn < ngroups && hn <= rdy) {
+        if (gn * 32 + (int)lane < n) rn = load_request(reqs + gn * 32 + lane);
+        have = true;
+      }
       WorkItem w;
       unsigned cnt = 0;
       if (i < n) plan_one(c, r, i, chunk, bctl, w, cnt);
@@ -521,8 +581,14 @@ __global__ void __launch_bounds__(256) batch_stream_kernel(Cfg c, const nvshmemx
       // pattern: fence, then strong stores); consumers acquire the tag
       __threadfence();
       for (unsigned k = 0; k < last; ++k) st_relaxed_b32(item_tag(items + first + k), gen);
+      g = gn;
+      if (g < ngroups && !have) {
+        ok_ready = hn <= rdy || refresh(hn);
+        if (ok_ready && g * 32 + (int)lane < n) rn = load_request(reqs + g * 32 + lane);
+      }
       r = rn;
     }
+    if (!ok_ready && lane == 0 && atomicCAS(&ctl->status, 0, NVSHMEMX_ERR_TIMEOUT) == 0) ctl->bad_request = -3;
     __syncwarp();
     if (lane == 0) {
       __threadfence();
@@ -562,10 +628,13 @@ __global__ void stream_reset_kernel(StreamCtl *ctl) {
   ctl->status = 0;
   ctl->bad_request = 0;
   ctl->plan_done = 0;
+  ctl->reqs_ready = 0;
+  ctl->plan_cursor = 0;
   ctl->gen = g == 0 ? 1u : g;
 }
 
-typedef void (*TmaFn)(const WorkItem *, BatchCtl *, unsigned long long, int, unsigned, unsigned, long long);
+typedef void (*TmaFn)(const WorkItem *, BatchCtl *, BatchCtl *, unsigned long long, int, unsigned, unsigned,
+                      long long);
 
 static TmaFn pick_tma(int stages) {
   switch (stages) {
@@ -585,7 +654,7 @@ static size_t tma_smem_bytes(const nvshmemx_batch_config &k) {
 static cudaError_t launch_stream(int stages, dim3 grid, dim3 block, size_t smem, cudaStream_t st, const Cfg &c,
                                  const nvshmemx_request *src, int n, unsigned chunk, WorkItem *items,
                                  unsigned long long cap, StreamCtl *ctl, int grab, unsigned SB, unsigned min_bulk,
-                                 int planners) {
+                                 int planners, const unsigned *ready, int resident0) {
   cudaLaunchConfig_t lc = {};
   lc.gridDim = grid;
   lc.blockDim = block;
@@ -597,9 +666,9 @@ static cudaError_t launch_stream(int stages, dim3 grid, dim3 block, size_t smem,
   lc.attrs = attr;
   lc.numAttrs = 1;
   switch (stages) {
-    case 2: return cudaLaunchKernelEx(&lc, batch_stream_kernel<2>, c, src, n, chunk, items, cap, ctl, grab, SB, min_bulk, planners);
-    case 3: return cudaLaunchKernelEx(&lc, batch_stream_kernel<3>, c, src, n, chunk, items, cap, ctl, grab, SB, min_bulk, planners);
-    case 4: return cudaLaunchKernelEx(&lc, batch_stream_kernel<4>, c, src, n, chunk, items, cap, ctl, grab, SB, min_bulk, planners);
+    case 2: return cudaLaunchKernelEx(&lc, batch_stream_kernel<2>, c, src, n, chunk, items, cap, ctl, grab, SB, min_bulk, planners, ready, resident0);
+    case 3: return cudaLaunchKernelEx(&lc, batch_stream_kernel<3>, c, src, n, chunk, items, cap, ctl, grab, SB, min_bulk, planners, ready, resident0);
+    case 4: return cudaLaunchKernelEx(&lc, batch_stream_kernel<4>, c, src, n, chunk, items, cap, ctl, grab, SB, min_bulk, planners, ready, resident0);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -613,7 +682,7 @@ static const void *stream_fn(int stages) {
   }
 }
 
-typedef void (*ExecFn)(const WorkItem *, BatchCtl *, unsigned long long, int);
+typedef void (*ExecFn)(const WorkItem *, BatchCtl *, const BatchCtl *, unsigned long long, int);
 
 static ExecFn pick_exec(int vb, int u) {
 #define NVSHM_PICK(V, UU) \
@@ -659,11 +728,12 @@ struct nvshmemx_batch {
   WorkItem *d_items = nullptr;
   BatchCtl *d_ctl = nullptr;
   nvshmemx_request *h_reqs = nullptr;  // pinned
-  const nvshmemx_request *h_reqs_dev = nullptr;  // h_reqs as the device sees it
   int *h_status = nullptr;             // pinned
   int n = 0;
   nvshmemx_batch_config cfg{};
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // staged submit: request pieces
+  cudaEvent_t ev_reset = nullptr, ev_copied = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   int graph_n = -1;
@@ -672,7 +742,23 @@ struct nvshmemx_batch {
   Cfg graph_arena{};
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr, ev_plan0 = nullptr, ev_exec0 = nullptr, ev_exec1 = nullptr;
   bool timed_direct = false;  // ev_plan0/ev_exec0/ev_exec1 hold the last direct execution
+  bool last_split = false;    // the last execution was a two-piece submit
 };
+
+// Control block of the second piece of a pipelined submit: bytes 64..95 of
+// the batch's 128-byte control allocation (bytes 32..63 hold the streaming
+// generation, which must never be zeroed).
+static BatchCtl *second_ctl(nvshmemx_batch *b) {
+  return reinterpret_cast<BatchCtl *>(reinterpret_cast<char *>(b->d_ctl) + 64);
+}
+
+// First-piece size of a pipelined submit: a quarter of the batch, in whole
+// 256-request plan blocks; 0 (one piece) below 8192 requests, where the copy
+// is too short to be worth hiding.
+static int split_point(int n) {
+  if (n < 8192) return 0;
+  return (n / 4) & ~255;
+}
 
 static void drop_graph(nvshmemx_batch *b) {
   if (b->gexec) cudaGraphExecDestroy(b->gexec);
@@ -682,34 +768,113 @@ static void drop_graph(nvshmemx_batch *b) {
   b->graph_n = -1;
 }
 
-// Enqueues memset + plan + exec (or, in stream mode, reset + the streaming
-// kernel) reading the requests at `src` on b->stream (used both for capture
-// and for the direct path).
-static int enqueue_batch(nvshmemx_batch *b, bool with_events, const nvshmemx_request *src) {
+// Resolved on first use: writes a 32-bit value from a stream's queue (no SM
+// involved) after the stream's earlier work, with a memory barrier before it.
+static PFN_cuStreamWriteValue32_v11070 g_write_value32 = nullptr;
+
+static int load_write_value() {
+  if (g_write_value32) return 0;
+  cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+  void *fn = nullptr;
+  if (cudaGetDriverEntryPointByVersion("cuStreamWriteValue32", &fn, 11070, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !fn)
+    return fail(NVSHMEMX_ERR_CUDA, "cannot resolve cuStreamWriteValue32");
+  g_write_value32 = reinterpret_cast<PFN_cuStreamWriteValue32_v11070>(fn);
+  return 0;
+}
+
+// Request pieces of a staged submit: a first piece of 8192 requests (256 KiB,
+// enough work to cover the arrival of the next), then doubling (few host
+// calls); every boundary but the last is a multiple of 32, the planners'
+// group size.
+static int staged_pieces(int n, int *ends, int max_pieces) {
+  int np = 0, at = 0, len = 8192;
+  while (at < n && np < max_pieces - 1) {
+    at = n - at > len ? at + len : n;
+    ends[np++] = at;
+    len *= 2;
+  }
+  if (at < n) ends[np++] = n;
+  return np;
+}
+
+// Stream mode: reset + the streaming kernel reading the requests at `src`.
+// With `host` set (staged submit) the requests are copied from there to
+// `src` in pieces on the copy stream while the kernel already runs; after
+// each piece the copy stream publishes the resident count in
+// ctl->reqs_ready, which the planners wait for.
+static int enqueue_stream(nvshmemx_batch *b, bool with_events, const nvshmemx_request *src,
+                          const nvshmemx_request *host, int n_host) {
   const Runtime &r = rt();
   const Cfg c = r.cfg;
   const nvshmemx_batch_config &k = b->cfg;
-  if (k.stream) {
-    const void *sfn = stream_fn(k.tma_stages);
-    if (!sfn) return fail(NVSHMEMX_ERR_INVALID, "batch: no streaming kernel for %d stages", k.tma_stages);
-    (void)cudaGetLastError();
-    const size_t smem = tma_smem_bytes(k);
-    cudaFuncSetAttribute(sfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sfn, k.threads, smem);
-    if (per_sm < 1) return fail(NVSHMEMX_ERR_COOP, "batch: streaming kernel does not fit an SM");
-    const int ctas = k.ctas_per_sm > 0 && k.ctas_per_sm < per_sm ? k.ctas_per_sm : per_sm;
-    StreamCtl *sctl = reinterpret_cast<StreamCtl *>(b->d_ctl);
-    if (with_events) cudaEventRecord(b->ev_plan0, b->stream);
-    stream_reset_kernel<<<1, 1, 0, b->stream>>>(sctl);
-    if (with_events) cudaEventRecord(b->ev_exec0, b->stream);
-    cudaError_t e = launch_stream(k.tma_stages, dim3(r.sm_count * ctas), dim3(k.threads), smem, b->stream, c, src,
-                                  b->n, (unsigned)k.chunk_bytes, b->d_items, b->cap, sctl, k.grab,
-                                  (unsigned)k.tma_stage_bytes, (unsigned)k.tma_min_bytes, k.stream_planners);
-    if (with_events) cudaEventRecord(b->ev_exec1, b->stream);
-    if (e != cudaSuccess) return check_cuda(e, "batch streaming launch");
-    return check_cuda(cudaGetLastError(), "batch streaming launch");
+  const void *sfn = stream_fn(k.tma_stages);
+  if (!sfn) return fail(NVSHMEMX_ERR_INVALID, "batch: no streaming kernel for %d stages", k.tma_stages);
+  int rc;
+  if (host && (rc = load_write_value())) return rc;
+  (void)cudaGetLastError();
+  const size_t smem = tma_smem_bytes(k);
+  cudaFuncSetAttribute(sfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sfn, k.threads, smem);
+  if (per_sm < 1) return fail(NVSHMEMX_ERR_COOP, "batch: streaming kernel does not fit an SM");
+  const int ctas = k.ctas_per_sm > 0 && k.ctas_per_sm < per_sm ? k.ctas_per_sm : per_sm;
+  StreamCtl *sctl = reinterpret_cast<StreamCtl *>(b->d_ctl);
+  if (with_events) cudaEventRecord(b->ev_plan0, b->stream);
+  stream_reset_kernel<<<1, 1, 0, b->stream>>>(sctl);
+  if (with_events) cudaEventRecord(b->ev_exec0, b->stream);
+  int ends[32];
+  const int np = host ? staged_pieces(n_host, ends, 32) : 0;
+  // piece p on stream `st`: the copy, then (pieces after the first) the
+  // resident count, published by the stream itself (no SM involved)
+  auto piece = [&](int p, cudaStream_t st) -> int {
+    const int at = p ? ends[p - 1] : 0;
+    int prc = check_cuda(cudaMemcpyAsync(const_cast<nvshmemx_request *>(src) + at, host + at,
+                                         (size_t)(ends[p] - at) * sizeof(nvshmemx_request), cudaMemcpyHostToDevice,
+                                         st),
+                         "cudaMemcpyAsync(request piece)");
+    if (prc || p == 0) return prc;
+    CUresult ce = g_write_value32(st, (CUdeviceptr)&sctl->reqs_ready, (cuuint32_t)ends[p],
+                                  CU_STREAM_WRITE_VALUE_DEFAULT);
+    return ce == CUDA_SUCCESS ? 0 : fail(NVSHMEMX_ERR_CUDA, "cuStreamWriteValue32 failed (%d)", (int)ce);
+  };
+  if (np) {
+    // The first piece goes ahead of the kernel on the batch's stream, so the
+    // kernel starts with it resident; the others follow on the copy stream
+    // once the reset (which zeroes reqs_ready) and the first piece are done.
+    if ((rc = piece(0, b->stream)) ||
+        (rc = check_cuda(cudaEventRecord(b->ev_reset, b->stream), "cudaEventRecord")) ||
+        (rc = check_cuda(cudaStreamWaitEvent(b->copy_stream, b->ev_reset, 0), "cudaStreamWaitEvent")))
+      return rc;
+    // queue the second piece before the launch: a failure to queue it
+    // leaves no kernel waiting for it
+    if (np > 1 && (rc = piece(1, b->copy_stream))) return rc;
   }
+  cudaError_t e = launch_stream(k.tma_stages, dim3(r.sm_count * ctas), dim3(k.threads), smem, b->stream, c, src,
+                                b->n, (unsigned)k.chunk_bytes, b->d_items, b->cap, sctl, k.grab,
+                                (unsigned)k.tma_stage_bytes, (unsigned)k.tma_min_bytes, k.stream_planners,
+                                np ? &sctl->reqs_ready : nullptr, np ? ends[0] : 0);
+  if (e != cudaSuccess) return check_cuda(e, "batch streaming launch");
+  if (np > 1) {
+    for (int p = 2; p < np; ++p)
+      if ((rc = piece(p, b->copy_stream))) return rc;
+    // later work on the batch's stream comes after the copies
+    if ((rc = check_cuda(cudaEventRecord(b->ev_copied, b->copy_stream), "cudaEventRecord")) ||
+        (rc = check_cuda(cudaStreamWaitEvent(b->stream, b->ev_copied, 0), "cudaStreamWaitEvent")))
+      return rc;
+  }
+  if (with_events) cudaEventRecord(b->ev_exec1, b->stream);
+  return check_cuda(cudaGetLastError(), "batch streaming launch");
+}
+
+// Plan + exec of one piece of a batch (n requests at `src`) on stream `st`,
+// with the piece's control block `ctl`, errors into `sctl`, and the items
+// appended after those of `prev` (nullptr: the first piece).
+static int enqueue_piece(nvshmemx_batch *b, bool with_events, const nvshmemx_request *src, int n, BatchCtl *ctl,
+                         BatchCtl *sctl, const BatchCtl *prev, int req_base, cudaStream_t st) {
+  const Runtime &r = rt();
+  const Cfg c = r.cfg;
+  const nvshmemx_batch_config &k = b->cfg;
   ExecFn fn = pick_exec(k.vec_bytes, k.unroll);
   TmaFn tfn = k.tma_stages ? pick_tma(k.tma_stages) : nullptr;
   if (!fn || (k.tma_stages && !tfn))
@@ -726,20 +891,28 @@ static int enqueue_batch(nvshmemx_batch *b, bool with_events, const nvshmemx_req
   }
   if (per_sm < 1) per_sm = 1;
   int ctas = k.ctas_per_sm > 0 && k.ctas_per_sm < per_sm ? k.ctas_per_sm : per_sm;
-  cudaMemsetAsync(b->d_ctl, 0, sizeof(BatchCtl), b->stream);
-  if (with_events) cudaEventRecord(b->ev_plan0, b->stream);
-  if (b->n > 0)
-    batch_plan_kernel<<<(b->n + 255) / 256, 256, 0, b->stream>>>(c, src, b->n, (unsigned)k.chunk_bytes,
-                                                                 b->d_items, b->cap, b->d_ctl);
-  if (with_events) cudaEventRecord(b->ev_exec0, b->stream);
+  if (with_events) cudaEventRecord(b->ev_plan0, st);
+  if (n > 0)
+    batch_plan_kernel<<<(n + 255) / 256, 256, 0, st>>>(c, src, n, (unsigned)k.chunk_bytes, b->d_items, b->cap, ctl,
+                                                       sctl, prev, req_base);
+  if (with_events) cudaEventRecord(b->ev_exec0, st);
   if (tfn)
-    tfn<<<r.sm_count * ctas, k.threads, smem, b->stream>>>(b->d_items, b->d_ctl, b->cap, k.grab,
-                                                             (unsigned)k.tma_stage_bytes, (unsigned)k.tma_min_bytes,
-                                                             c.wait_timeout_ns);
+    tfn<<<r.sm_count * ctas, k.threads, smem, st>>>(b->d_items, ctl, sctl, b->cap, k.grab,
+                                                      (unsigned)k.tma_stage_bytes, (unsigned)k.tma_min_bytes,
+                                                      c.wait_timeout_ns);
   else
-    fn<<<r.sm_count * ctas, k.threads, 0, b->stream>>>(b->d_items, b->d_ctl, b->cap, k.grab);
-  if (with_events) cudaEventRecord(b->ev_exec1, b->stream);
+    fn<<<r.sm_count * ctas, k.threads, 0, st>>>(b->d_items, ctl, sctl, b->cap, k.grab);
+  if (with_events) cudaEventRecord(b->ev_exec1, st);
   return check_cuda(cudaGetLastError(), "batch launch");
+}
+
+// Enqueues memset + plan + exec (or, in stream mode, reset + the streaming
+// kernel) reading the requests at `src` on b->stream (used both for capture
+// and for the direct path).
+static int enqueue_batch(nvshmemx_batch *b, bool with_events, const nvshmemx_request *src) {
+  if (b->cfg.stream) return enqueue_stream(b, with_events, src, nullptr, 0);
+  cudaMemsetAsync(b->d_ctl, 0, sizeof(BatchCtl), b->stream);
+  return enqueue_piece(b, with_events, src, b->n, b->d_ctl, b->d_ctl, nullptr, 0, b->stream);
 }
 
 static int ensure_graph(nvshmemx_batch *b, const nvshmemx_request *src) {
@@ -808,7 +981,8 @@ int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes
       (rc = check_cuda(cudaMallocHost(&b->h_reqs, (size_t)max_requests * sizeof(nvshmemx_request)),
                        "cudaMallocHost(reqs)")) ||
       (rc = check_cuda(cudaMallocHost(&b->h_status, 64), "cudaMallocHost(status)")) ||
-      (rc = check_cuda(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate"))) {
+      (rc = check_cuda(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate")) ||
+      (rc = check_cuda(cudaStreamCreateWithFlags(&b->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate"))) {
     nvshmemx_batch_destroy(b);
     return rc;
   }
@@ -817,16 +991,12 @@ int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes
   cudaEventCreate(&b->ev_plan0);
   cudaEventCreate(&b->ev_exec0);
   cudaEventCreate(&b->ev_exec1);
+  cudaEventCreateWithFlags(&b->ev_reset, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&b->ev_copied, cudaEventDisableTiming);
   // control block (BatchCtl or StreamCtl) and every work item's generation
   // tag start at zero; streaming generations start at 1
   cudaMemset(b->d_ctl, 0, 128);
   cudaMemset(b->d_items, 0, (size_t)b->cap * sizeof(WorkItem));
-  void *dev_alias = nullptr;
-  if ((rc = check_cuda(cudaHostGetDevicePointer(&dev_alias, b->h_reqs, 0), "cudaHostGetDevicePointer"))) {
-    nvshmemx_batch_destroy(b);
-    return rc;
-  }
-  b->h_reqs_dev = static_cast<const nvshmemx_request *>(dev_alias);
   *out = b;
   return 0;
 }
@@ -834,16 +1004,18 @@ int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes
 int nvshmemx_batch_destroy(nvshmemx_batch *b) {
   if (!b) return 0;
   if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->copy_stream) cudaStreamSynchronize(b->copy_stream);
   drop_graph(b);
   if (b->d_reqs) cudaFree(b->d_reqs);
   if (b->d_items) cudaFree(b->d_items);
   if (b->d_ctl) cudaFree(b->d_ctl);
   if (b->h_reqs) cudaFreeHost(b->h_reqs);
   if (b->h_status) cudaFreeHost(b->h_status);
-  cudaEvent_t evs[] = {b->ev_start, b->ev_stop, b->ev_plan0, b->ev_exec0, b->ev_exec1};
+  cudaEvent_t evs[] = {b->ev_start, b->ev_stop, b->ev_plan0, b->ev_exec0, b->ev_exec1, b->ev_reset, b->ev_copied};
   for (auto e : evs)
     if (e) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);
+  if (b->copy_stream) cudaStreamDestroy(b->copy_stream);
   delete b;
   return 0;
 }
@@ -879,6 +1051,7 @@ int nvshmemx_batch_execute(nvshmemx_batch *b, int reps, float *out_ms) {
   if (!b || reps < 1) return fail(NVSHMEMX_ERR_INVALID, "batch_execute: bad arguments");
   int rc;
   if ((rc = ensure_graph(b, b->d_reqs))) return rc;
+  b->last_split = false;
   cudaEventRecord(b->ev_start, b->stream);
   for (int i = 0; i < reps; ++i)
     if ((rc = check_cuda(cudaGraphLaunch(b->gexec, b->stream), "cudaGraphLaunch"))) return rc;
@@ -894,21 +1067,53 @@ int nvshmemx_batch_execute(nvshmemx_batch *b, int reps, float *out_ms) {
 }
 
 int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n, int *out_status, float *out_ms) {
-  if (!b || n < 0 || n > b->max_n) return fail(NVSHMEMX_ERR_INVALID, "batch_submit: n outside [0, max]");
+  if (!b || n < 0 || n > b->max_n || (n && !reqs)) return fail(NVSHMEMX_ERR_INVALID, "batch_submit: bad arguments");
   int rc;
   b->n = n;
-  // In stream mode the batch's own pinned buffer is read by the kernel over
-  // the host link while execution is already running; any other source is
-  // first copied to device memory.
-  const bool zero_copy = b->cfg.stream && reqs == b->h_reqs;
-  if ((rc = ensure_graph(b, zero_copy ? b->h_reqs_dev : b->d_reqs))) return rc;
+  const bool staged = b->cfg.stream && n > 0;
+  const int n0 = staged ? 0 : split_point(n);
+  if (!staged && !n0 && (rc = ensure_graph(b, b->d_reqs))) return rc;
+  b->last_split = n0 > 0;
+  b->timed_direct = false;
   cudaEventRecord(b->ev_start, b->stream);
-  if (n && !zero_copy &&
-      (rc = check_cuda(cudaMemcpyAsync(b->d_reqs, reqs, (size_t)n * sizeof(nvshmemx_request), cudaMemcpyHostToDevice,
-                                       b->stream),
-                       "cudaMemcpyAsync(requests)")))
-    return rc;
-  if ((rc = check_cuda(cudaGraphLaunch(b->gexec, b->stream), "cudaGraphLaunch"))) return rc;
+  if (staged) {
+    // stream mode: the kernel starts at once and plans each piece of the
+    // requests as the copy stream lands it
+    if ((rc = enqueue_stream(b, false, b->d_reqs, reqs, n))) {
+      cudaStreamSynchronize(b->copy_stream);
+      cudaStreamSynchronize(b->stream);
+      return rc;
+    }
+  } else if (n0) {
+    // Two pieces: the first quarter is copied, planned and executed while
+    // the copy stream brings the rest; the second piece is planned (its
+    // items appended after the first's) and executed once both are done.
+    BatchCtl *c0 = b->d_ctl, *c1 = second_ctl(b);
+    if ((rc = check_cuda(cudaMemsetAsync(c0, 0, sizeof(BatchCtl), b->stream), "cudaMemsetAsync")) ||
+        (rc = check_cuda(cudaMemsetAsync(c1, 0, sizeof(BatchCtl), b->stream), "cudaMemsetAsync")) ||
+        (rc = check_cuda(cudaMemcpyAsync(b->d_reqs, reqs, (size_t)n0 * sizeof(nvshmemx_request),
+                                         cudaMemcpyHostToDevice, b->stream),
+                         "cudaMemcpyAsync(requests)")) ||
+        (rc = check_cuda(cudaEventRecord(b->ev_reset, b->stream), "cudaEventRecord")) ||
+        (rc = check_cuda(cudaStreamWaitEvent(b->copy_stream, b->ev_reset, 0), "cudaStreamWaitEvent")) ||
+        (rc = check_cuda(cudaMemcpyAsync(b->d_reqs + n0, reqs + n0, (size_t)(n - n0) * sizeof(nvshmemx_request),
+                                         cudaMemcpyHostToDevice, b->copy_stream),
+                         "cudaMemcpyAsync(requests)")) ||
+        (rc = check_cuda(cudaEventRecord(b->ev_copied, b->copy_stream), "cudaEventRecord")) ||
+        (rc = enqueue_piece(b, false, b->d_reqs, n0, c0, c0, nullptr, 0, b->stream)) ||
+        (rc = check_cuda(cudaStreamWaitEvent(b->stream, b->ev_copied, 0), "cudaStreamWaitEvent")) ||
+        (rc = enqueue_piece(b, false, b->d_reqs + n0, n - n0, c1, c0, c0, n0, b->stream))) {
+      cudaStreamSynchronize(b->copy_stream);
+      cudaStreamSynchronize(b->stream);
+      return rc;
+    }
+  } else {
+    if (n && (rc = check_cuda(cudaMemcpyAsync(b->d_reqs, reqs, (size_t)n * sizeof(nvshmemx_request),
+                                              cudaMemcpyHostToDevice, b->stream),
+                              "cudaMemcpyAsync(requests)")))
+      return rc;
+    if ((rc = check_cuda(cudaGraphLaunch(b->gexec, b->stream), "cudaGraphLaunch"))) return rc;
+  }
   if ((rc = check_cuda(cudaMemcpyAsync(b->h_status, &b->d_ctl->status, 8, cudaMemcpyDeviceToHost, b->stream),
                        "cudaMemcpyAsync(status)")))
     return rc;
@@ -924,10 +1129,10 @@ int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n
 int nvshmemx_batch_last_stats(const nvshmemx_batch *b, unsigned long long *chunks, float *plan_ms, float *exec_ms) {
   if (!b) return NVSHMEMX_ERR_INVALID;
   if (chunks) {
-    BatchCtl h;
-    if (cudaMemcpy(&h, b->d_ctl, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess)
+    BatchCtl h[3];  // bytes 0..95: first piece, (streaming state), second piece
+    if (cudaMemcpy(h, b->d_ctl, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess)
       return check_cuda(cudaGetLastError(), "batch_last_stats");
-    *chunks = h.total_chunks;
+    *chunks = h[0].total_chunks + (b->last_split ? h[2].total_chunks : 0ull);
   }
   float p = 0, e = 0;
   if (b->timed_direct) {
@@ -947,6 +1152,7 @@ int nvshmemx_batch_execute_direct(nvshmemx_batch *b, int reps, float *out_ms, fl
   if (!b || reps < 1) return fail(NVSHMEMX_ERR_INVALID, "batch_execute_direct: bad arguments");
   int rc;
   float total = 0, exec = 0;
+  b->last_split = false;
   for (int i = 0; i < reps; ++i) {
     cudaEventRecord(b->ev_start, b->stream);
     if ((rc = enqueue_batch(b, true, b->d_reqs))) return rc;
@@ -1082,12 +1288,12 @@ extern "C" int nvshmemx_batch_execute_noalloc(const nvshmemx_request *d_reqs, in
   if ((rc = check_cuda(cudaMemsetAsync(ctl, 0, sizeof(BatchCtl), s), "cudaMemsetAsync(noalloc control)"))) return rc;
   if (n > 0)
     batch_plan_kernel<<<(n + 255) / 256, 256, 0, s>>>(r.cfg, d_reqs, n, (unsigned)k.chunk_bytes, items,
-                                                      kNoallocMaxItems, ctl);
+                                                      kNoallocMaxItems, ctl, ctl, nullptr, 0);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, k.threads, 0);
   if (per_sm < 1) per_sm = 1;
   const int ctas = k.ctas_per_sm > 0 && k.ctas_per_sm < per_sm ? k.ctas_per_sm : per_sm;
-  fn<<<r.sm_count * ctas, k.threads, 0, s>>>(items, ctl, kNoallocMaxItems, k.grab);
+  fn<<<r.sm_count * ctas, k.threads, 0, s>>>(items, ctl, ctl, kNoallocMaxItems, k.grab);
   if ((rc = check_cuda(cudaGetLastError(), "batch_execute_noalloc launch"))) return rc;
   int st[2] = {0, 0};
   if ((rc = check_cuda(cudaMemcpyAsync(st, &ctl->status, sizeof st, cudaMemcpyDeviceToHost, s),

@@ -83,9 +83,20 @@ int nvshmemx_batch_upload(nvshmemx_batch *b, const nvshmemx_request *reqs, int n
 int nvshmemx_batch_execute(nvshmemx_batch *b, int reps, float *out_ms);
 
 /* End-to-end call: copies n requests from host memory (pinned if it is the
- * batch's host buffer), executes them and reads back the batch status word,
- * all on the batch's stream; *out_status receives the status (0 = every
- * request done), *out_ms the device time of the whole sequence. */
+ * batch's host buffer), executes them and reads back the batch status word;
+ * *out_status receives the status (0 = every request done), *out_ms the
+ * device time of the whole sequence.  With a graph configuration (stream 0)
+ * the copy precedes the plan and exec kernels on the batch's stream; from
+ * 8192 requests on, the batch runs as two pieces: the first quarter (in
+ * whole 256-request blocks) is copied, planned and executed while a second
+ * stream copies the rest, which is then planned and executed.  An invalid
+ * request in the second piece is reported after the first piece has run
+ * (with one piece, nothing runs).  In
+ * stream mode the streaming kernel is launched first and the requests are
+ * copied in growing pieces (2048, 4096, ... requests) on a second stream,
+ * each piece followed by a stream write of the resident count that the
+ * kernel's planners wait for, so the copy overlaps execution.  The requests
+ * stay resident: nvshmemx_batch_execute afterwards runs the same batch. */
 int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n, int *out_status,
                           float *out_ms);
 

@@ -108,34 +108,84 @@ def test_submit_end_to_end(shmem_factory):
     assert first_diff(heap_images(sh, npes, heap), om.heap) is None
 
 
-def test_stream_submit_reads_pinned_host_buffer(shmem_factory):
-    """End-to-end in stream mode: the kernel reads the requests from the
-    batch's pinned host buffer while it executes; two different batches in a
-    row through the same buffer (generation tags keep them apart)."""
-    npes, heap = 8, 8 << 20
+@pytest.mark.parametrize("cfg", [None, CONFIGS[0]], ids=["tma", "register"])
+def test_submit_pipelined_two_pieces(shmem_factory, cfg):
+    """A submit of 8192 or more requests in a graph configuration runs in two
+    pieces: the first quarter executes while the rest is copied, and the
+    second piece's chunks are appended after the first's."""
+    npes, heap = 16, 16 << 20
+    reqs = c4_batch(seed=48, n=20000, npes=npes, heap=heap, hi=16 << 10)
     sh, om = setup(shmem_factory, npes, heap)
-    with sh.batch(4000, 64 << 20, 4096) as b:
+    with sh.batch(len(reqs), int(reqs["bytes"].sum()), 256) as b:
+        if cfg:
+            b.set_config(cfg)
+        buf = b.host_buffer()
+        buf[:] = reqs
+        st, ms = b.submit(buf, len(reqs))
+        assert st == 0 and ms > 0
+        chunks = b.stats()[0]
+        om.apply_requests(reqs)
+        assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+        # the requests stay resident; one-piece execution plans the same chunks
+        b.execute(1)
+        assert b.stats()[0] == chunks
+        assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+        # a bad request in the second piece: the first piece has run, the
+        # second has not
+        n0 = (len(reqs) // 4) & ~255
+        for pe in range(npes):
+            sh.fill_random(pe, 0, heap, 8)
+        om2 = Model(npes, heap)
+        for pe in range(npes):
+            om2.fill_random(pe, 0, heap, 8)
+        bad = reqs.copy()
+        bad[n0 + 100]["dst_pe"] = 99
+        st, _ = b.submit(bad)
+        assert st == ERR_BOUNDS
+        om2.apply_requests(reqs[:n0])
+        assert first_diff(heap_images(sh, npes, heap), om2.heap) is None
+    sh.status()
+
+
+def test_stream_submit_staged_pieces(shmem_factory):
+    """End-to-end in stream mode: the streaming kernel starts at once and
+    plans each piece of the requests as the copy stream lands it (8192,
+    16384, 32768, ... requests per piece).  Batches of several sizes in a row
+    (three pieces, two, one) through the pinned buffer and from ordinary
+    (pageable) host memory."""
+    npes, heap = 16, 16 << 20
+    sh, om = setup(shmem_factory, npes, heap)
+    with sh.batch(30000, 256 << 20, 4096) as b:
         b.set_config(STREAM)
         buf = b.host_buffer()
-        for seed in (41, 42):
-            reqs = c4_batch(seed=seed, n=3000, npes=npes, heap=heap, hi=128 << 10)
-            buf[:len(reqs)] = reqs
-            st, ms = b.submit(buf, len(reqs))
+        for seed, n, pinned in ((41, 30000, True), (42, 9000, False), (46, 777, False), (47, 8192, True)):
+            reqs = c4_batch(seed=seed, n=n, npes=npes, heap=heap, hi=16 << 10)
+            if pinned:
+                buf[:len(reqs)] = reqs
+                st, ms = b.submit(buf, len(reqs))
+            else:
+                st, ms = b.submit(reqs.copy())
             assert st == 0 and ms > 0
             om.apply_requests(reqs)
-            assert first_diff(heap_images(sh, npes, heap), om.heap) is None
-        # device-resident execution of the same object (graph of the stream kernel)
-        reqs = c4_batch(seed=43, n=2500, npes=npes, heap=heap, hi=128 << 10)
-        b.upload(reqs)
+            assert first_diff(heap_images(sh, npes, heap), om.heap) is None, (seed, n)
+        # the staged requests stay resident: device-resident execution (the
+        # graph of the streaming kernel) of the last batch
         b.execute(2)
         om.apply_requests(reqs)
         assert first_diff(heap_images(sh, npes, heap), om.heap) is None
         # switching between graph and stream modes on one object stays exact
+        reqs = c4_batch(seed=43, n=2500, npes=npes, heap=heap, hi=128 << 10)
+        b.upload(reqs)
         b.set_config(dict(STREAM, stream=0))
         b.execute(1)
         b.set_config(STREAM)
         b.execute(1)
+        om.apply_requests(reqs)
+        om.apply_requests(reqs)
         assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+        # an empty staged submit does nothing
+        st, _ = b.submit(buf, 0)
+        assert st == 0
     assert sh.status() == 0
 
 
