@@ -182,17 +182,6 @@ def load_tuned():
     return None
 
 
-def load_tuned_stream():
-    """Fastest streaming-mode row of the tuned table (plan and execute in one
-    launch; the mode that reads host-resident requests without a copy)."""
-    if os.path.exists(TUNED):
-        with open(TUNED) as f:
-            rows = [r for r in json.load(f).get("results", []) if r["cfg"].get("stream") and r["status"] == 0]
-        if rows:
-            return min(rows, key=lambda r: r["ms_median"])["cfg"]
-    return None
-
-
 def run_extras(peak):
     """Latency metrics (C1 ping-pong, device barrier on 8 PEs) and C2 bulk
     all-to-all throughput (8 PEs, rotating buffer sets larger than 2x L2)."""
@@ -409,28 +398,6 @@ def run_gpu(args, rank, world, local):
                 barrier(dist)
                 t_e2e = reduce_max(dist, sum(e2e_ms) / 1e3)
                 cfg_used = b.config()
-                # the same call in streaming mode: the kernel reads the pinned
-                # request buffer over the host link while it executes
-                # (8192 or more requests in a graph configuration: two pieces,
-                # the first quarter executing while the rest is copied)
-                e2e_modes = {"pipelined": t_e2e}
-                scfg = load_tuned_stream()
-                if scfg:
-                    b.set_config(scfg)
-                    for _ in range(args.warmup):
-                        flush()
-                        b.submit(hb, len(reqs))
-                    barrier(dist)
-                    s_ms = []
-                    for _ in range(args.steps):
-                        flush()
-                        st, ms = b.submit(hb, len(reqs))
-                        assert st == 0, f"batch status {st}"
-                        s_ms.append(ms)
-                    barrier(dist)
-                    e2e_modes["stream"] = reduce_max(dist, sum(s_ms) / 1e3)
-                e2e_mode = min(e2e_modes, key=e2e_modes.get)
-                t_e2e = e2e_modes[e2e_mode]
             assert sh.status() == 0
             checks = [sh.checksum(pe, 0, C4["heap"]) for pe in range(C4["npes"])]
         if args.only != "batch":
@@ -460,13 +427,11 @@ def run_gpu(args, rank, world, local):
         "percall_GBps": {k: round(v, 2) for k, v in pc.items()},
         "speedup_vs_percall_thread": round(value / pc["thread"], 2),
         "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(len(reqs) * 32),
-                "d2h_bytes_per_step": 8, "mode": e2e_mode,
-                "GBps_by_mode": {k: round(world * alg * args.steps / v / 1e9, 2) for k, v in e2e_modes.items()},
-                "stream_config": scfg},
+                "d2h_bytes_per_step": 8,
+                "mode": "pipelined: the first quarter of the requests executes while the rest is copied"},
         # plan + exec per device-resident step, 2 x (plan + exec) per
-        # pipelined end-to-end step, reset + streaming kernel per streaming
-        # end-to-end step
-        "gpu_launches": 2 * args.steps + 4 * args.steps + (2 * args.steps if scfg else 0),
+        # pipelined end-to-end step
+        "gpu_launches": 2 * args.steps + 4 * args.steps,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 3), "traffic": traffic,
                      "kernel": ("batch_exec_tma_kernel" if cfg_used.get("tma_stages") else "batch_exec_kernel"),

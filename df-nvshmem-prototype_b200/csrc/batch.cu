@@ -12,8 +12,6 @@
 //            chunk with VB-byte accesses, U in flight per lane.
 // Every chunk is a contiguous copy, so the exec kernel is pure streaming:
 // its roofline is HBM copy bandwidth (2 bytes moved per payload byte).
-#include <cuda.h>
-#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <string.h>
@@ -365,9 +363,8 @@ struct StreamCtl {                 // the first 32 bytes match BatchCtl
   unsigned int gen;                // generation of the current launch; outside
                                    // the 32 bytes the graph path zeroes, so it
                                    // only ever grows
-  unsigned int reqs_ready;         // staged submit: requests resident so far,
-                                   // written by the copy stream after each piece
   unsigned int plan_cursor;        // next group of 32 requests to plan
+  unsigned int pad1;
   unsigned long long pad[2];
 };
 static_assert(sizeof(StreamCtl) == 64, "StreamCtl is one 64-byte block");
@@ -488,8 +485,7 @@ template <int S>
 __global__ void __launch_bounds__(256) batch_stream_kernel(Cfg c, const nvshmemx_request *reqs, int n,
                                                            unsigned chunk, WorkItem *__restrict__ items,
                                                            unsigned long long cap, StreamCtl *ctl, int grab,
-                                                           unsigned SB, unsigned min_bulk, int planners_per_cta,
-                                                           const unsigned *ready, int resident0) {
+                                                           unsigned SB, unsigned min_bulk, int planners_per_cta) {
   extern __shared__ __align__(128) char smem[];
   const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   BatchCtl *bctl = reinterpret_cast<BatchCtl *>(ctl);
@@ -500,32 +496,8 @@ __global__ void __launch_bounds__(256) batch_stream_kernel(Cfg c, const nvshmemx
   // ---- planning (the first planners_per_cta warps of each CTA)
   if (warp < (unsigned)planners_per_cta) {
     const int ngroups = (n + 31) / 32;
-    // Requests known to be resident: all of them, or (staged submit) the
-    // first `resident0` plus the count the copy stream has published in
-    // *ready since, refreshed on demand.
-    int rdy = ready ? resident0 : n;
-    auto refresh = [&](int upto) -> bool {
-      int v = 0;
-      if (lane == 0) {
-        unsigned ns = 0;
-        for (unsigned spins = 0;; ++spins) {
-          v = ld_acquire(reinterpret_cast<const int *>(ready));
-          if (v >= upto) break;
-          ns = ns == 0 ? 64 : (ns >= 1024 ? 1024 : ns * 2);
-          __nanosleep(ns);
-          if ((spins & 15) == 15 && gtimer() > ring.deadline) {
-            v = -1;
-            break;
-          }
-        }
-      }
-      v = __shfl_sync(0xffffffffu, v, 0);
-      if (v < 0) return false;
-      rdy = v > rdy ? v : rdy;
-      return true;
-    };
-    // groups are claimed in request order, so planning follows the pieces
-    // as they land and items are published roughly in request order
+    // groups are claimed in request order, so items are published roughly
+    // in request order (the order in which executing warps claim them)
     auto claim = [&]() -> int {
       int v = 0;
       if (lane == 0) v = (int)atomicAdd(&ctl->plan_cursor, 1u);
@@ -533,24 +505,13 @@ __global__ void __launch_bounds__(256) batch_stream_kernel(Cfg c, const nvshmemx
     };
     int g = claim();
     nvshmemx_request r;
-    bool ok_ready = true;
-    if (g < ngroups) {
-      const int hi = g * 32 + 32 < n ? g * 32 + 32 : n;
-      ok_ready = hi <= rdy || refresh(hi);
-      if (ok_ready && g * 32 + (int)lane < n) r = load_request(reqs + g * 32 + lane);
-    }
-    for (; g < ngroups && ok_ready;) {
+    if (g < ngroups && g * 32 + (int)lane < n) r = load_request(reqs + g * 32 + lane);
+    while (g < ngroups) {
       const int i = g * 32 + (int)lane;
-      // claim the next group and fetch it while this one is planned, if it
-      // is resident already
+      // claim the next group and fetch it while this one is planned
       const int gn = claim();
       nvshmemx_request rn;
-      bool have = false;
-      const int hn = gn * 32 + 32 < n ? gn * 32 + 32 : n;
-      if (gn < ngroups && hn <= rdy) {
-        if (gn * 32 + (int)lane < n) rn = load_request(reqs + gn * 32 + lane);
-        have = true;
-      }
+      if (gn < ngroups && gn * 32 + (int)lane < n) rn = load_request(reqs + gn * 32 + lane);
       WorkItem w;
       unsigned cnt = 0;
       if (i < n) plan_one(c, r, i, chunk, bctl, w, cnt);
@@ -582,13 +543,8 @@ __global__ void __launch_bounds__(256) batch_stream_kernel(Cfg c, const nvshmemx
       __threadfence();
       for (unsigned k = 0; k < last; ++k) st_relaxed_b32(item_tag(items + first + k), gen);
       g = gn;
-      if (g < ngroups && !have) {
-        ok_ready = hn <= rdy || refresh(hn);
-        if (ok_ready && g * 32 + (int)lane < n) rn = load_request(reqs + g * 32 + lane);
-      }
       r = rn;
     }
-    if (!ok_ready && lane == 0 && atomicCAS(&ctl->status, 0, NVSHMEMX_ERR_TIMEOUT) == 0) ctl->bad_request = -3;
     __syncwarp();
     if (lane == 0) {
       __threadfence();
@@ -628,7 +584,6 @@ __global__ void stream_reset_kernel(StreamCtl *ctl) {
   ctl->status = 0;
   ctl->bad_request = 0;
   ctl->plan_done = 0;
-  ctl->reqs_ready = 0;
   ctl->plan_cursor = 0;
   ctl->gen = g == 0 ? 1u : g;
 }
@@ -654,7 +609,7 @@ static size_t tma_smem_bytes(const nvshmemx_batch_config &k) {
 static cudaError_t launch_stream(int stages, dim3 grid, dim3 block, size_t smem, cudaStream_t st, const Cfg &c,
                                  const nvshmemx_request *src, int n, unsigned chunk, WorkItem *items,
                                  unsigned long long cap, StreamCtl *ctl, int grab, unsigned SB, unsigned min_bulk,
-                                 int planners, const unsigned *ready, int resident0) {
+                                 int planners) {
   cudaLaunchConfig_t lc = {};
   lc.gridDim = grid;
   lc.blockDim = block;
@@ -666,9 +621,9 @@ static cudaError_t launch_stream(int stages, dim3 grid, dim3 block, size_t smem,
   lc.attrs = attr;
   lc.numAttrs = 1;
   switch (stages) {
-    case 2: return cudaLaunchKernelEx(&lc, batch_stream_kernel<2>, c, src, n, chunk, items, cap, ctl, grab, SB, min_bulk, planners, ready, resident0);
-    case 3: return cudaLaunchKernelEx(&lc, batch_stream_kernel<3>, c, src, n, chunk, items, cap, ctl, grab, SB, min_bulk, planners, ready, resident0);
-    case 4: return cudaLaunchKernelEx(&lc, batch_stream_kernel<4>, c, src, n, chunk, items, cap, ctl, grab, SB, min_bulk, planners, ready, resident0);
+    case 2: return cudaLaunchKernelEx(&lc, batch_stream_kernel<2>, c, src, n, chunk, items, cap, ctl, grab, SB, min_bulk, planners);
+    case 3: return cudaLaunchKernelEx(&lc, batch_stream_kernel<3>, c, src, n, chunk, items, cap, ctl, grab, SB, min_bulk, planners);
+    case 4: return cudaLaunchKernelEx(&lc, batch_stream_kernel<4>, c, src, n, chunk, items, cap, ctl, grab, SB, min_bulk, planners);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -732,7 +687,7 @@ struct nvshmemx_batch {
   int n = 0;
   nvshmemx_batch_config cfg{};
   cudaStream_t stream = nullptr;
-  cudaStream_t copy_stream = nullptr;  // staged submit: request pieces
+  cudaStream_t copy_stream = nullptr;  // pipelined submit: the second piece's copy
   cudaEvent_t ev_reset = nullptr, ev_copied = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -768,50 +723,13 @@ static void drop_graph(nvshmemx_batch *b) {
   b->graph_n = -1;
 }
 
-// Resolved on first use: writes a 32-bit value from a stream's queue (no SM
-// involved) after the stream's earlier work, with a memory barrier before it.
-static PFN_cuStreamWriteValue32_v11070 g_write_value32 = nullptr;
-
-static int load_write_value() {
-  if (g_write_value32) return 0;
-  cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
-  void *fn = nullptr;
-  if (cudaGetDriverEntryPointByVersion("cuStreamWriteValue32", &fn, 11070, cudaEnableDefault, &q) != cudaSuccess ||
-      q != cudaDriverEntryPointSuccess || !fn)
-    return fail(NVSHMEMX_ERR_CUDA, "cannot resolve cuStreamWriteValue32");
-  g_write_value32 = reinterpret_cast<PFN_cuStreamWriteValue32_v11070>(fn);
-  return 0;
-}
-
-// Request pieces of a staged submit: a first piece of 8192 requests (256 KiB,
-// enough work to cover the arrival of the next), then doubling (few host
-// calls); every boundary but the last is a multiple of 32, the planners'
-// group size.
-static int staged_pieces(int n, int *ends, int max_pieces) {
-  int np = 0, at = 0, len = 8192;
-  while (at < n && np < max_pieces - 1) {
-    at = n - at > len ? at + len : n;
-    ends[np++] = at;
-    len *= 2;
-  }
-  if (at < n) ends[np++] = n;
-  return np;
-}
-
 // Stream mode: reset + the streaming kernel reading the requests at `src`.
-// With `host` set (staged submit) the requests are copied from there to
-// `src` in pieces on the copy stream while the kernel already runs; after
-// each piece the copy stream publishes the resident count in
-// ctl->reqs_ready, which the planners wait for.
-static int enqueue_stream(nvshmemx_batch *b, bool with_events, const nvshmemx_request *src,
-                          const nvshmemx_request *host, int n_host) {
+static int enqueue_stream(nvshmemx_batch *b, bool with_events, const nvshmemx_request *src) {
   const Runtime &r = rt();
   const Cfg c = r.cfg;
   const nvshmemx_batch_config &k = b->cfg;
   const void *sfn = stream_fn(k.tma_stages);
   if (!sfn) return fail(NVSHMEMX_ERR_INVALID, "batch: no streaming kernel for %d stages", k.tma_stages);
-  int rc;
-  if (host && (rc = load_write_value())) return rc;
   (void)cudaGetLastError();
   const size_t smem = tma_smem_bytes(k);
   cudaFuncSetAttribute(sfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -823,46 +741,10 @@ static int enqueue_stream(nvshmemx_batch *b, bool with_events, const nvshmemx_re
   if (with_events) cudaEventRecord(b->ev_plan0, b->stream);
   stream_reset_kernel<<<1, 1, 0, b->stream>>>(sctl);
   if (with_events) cudaEventRecord(b->ev_exec0, b->stream);
-  int ends[32];
-  const int np = host ? staged_pieces(n_host, ends, 32) : 0;
-  // piece p on stream `st`: the copy, then (pieces after the first) the
-  // resident count, published by the stream itself (no SM involved)
-  auto piece = [&](int p, cudaStream_t st) -> int {
-    const int at = p ? ends[p - 1] : 0;
-    int prc = check_cuda(cudaMemcpyAsync(const_cast<nvshmemx_request *>(src) + at, host + at,
-                                         (size_t)(ends[p] - at) * sizeof(nvshmemx_request), cudaMemcpyHostToDevice,
-                                         st),
-                         "cudaMemcpyAsync(request piece)");
-    if (prc || p == 0) return prc;
-    CUresult ce = g_write_value32(st, (CUdeviceptr)&sctl->reqs_ready, (cuuint32_t)ends[p],
-                                  CU_STREAM_WRITE_VALUE_DEFAULT);
-    return ce == CUDA_SUCCESS ? 0 : fail(NVSHMEMX_ERR_CUDA, "cuStreamWriteValue32 failed (%d)", (int)ce);
-  };
-  if (np) {
-    // The first piece goes ahead of the kernel on the batch's stream, so the
-    // kernel starts with it resident; the others follow on the copy stream
-    // once the reset (which zeroes reqs_ready) and the first piece are done.
-    if ((rc = piece(0, b->stream)) ||
-        (rc = check_cuda(cudaEventRecord(b->ev_reset, b->stream), "cudaEventRecord")) ||
-        (rc = check_cuda(cudaStreamWaitEvent(b->copy_stream, b->ev_reset, 0), "cudaStreamWaitEvent")))
-      return rc;
-    // queue the second piece before the launch: a failure to queue it
-    // leaves no kernel waiting for it
-    if (np > 1 && (rc = piece(1, b->copy_stream))) return rc;
-  }
   cudaError_t e = launch_stream(k.tma_stages, dim3(r.sm_count * ctas), dim3(k.threads), smem, b->stream, c, src,
                                 b->n, (unsigned)k.chunk_bytes, b->d_items, b->cap, sctl, k.grab,
-                                (unsigned)k.tma_stage_bytes, (unsigned)k.tma_min_bytes, k.stream_planners,
-                                np ? &sctl->reqs_ready : nullptr, np ? ends[0] : 0);
+                                (unsigned)k.tma_stage_bytes, (unsigned)k.tma_min_bytes, k.stream_planners);
   if (e != cudaSuccess) return check_cuda(e, "batch streaming launch");
-  if (np > 1) {
-    for (int p = 2; p < np; ++p)
-      if ((rc = piece(p, b->copy_stream))) return rc;
-    // later work on the batch's stream comes after the copies
-    if ((rc = check_cuda(cudaEventRecord(b->ev_copied, b->copy_stream), "cudaEventRecord")) ||
-        (rc = check_cuda(cudaStreamWaitEvent(b->stream, b->ev_copied, 0), "cudaStreamWaitEvent")))
-      return rc;
-  }
   if (with_events) cudaEventRecord(b->ev_exec1, b->stream);
   return check_cuda(cudaGetLastError(), "batch streaming launch");
 }
@@ -910,7 +792,7 @@ static int enqueue_piece(nvshmemx_batch *b, bool with_events, const nvshmemx_req
 // kernel) reading the requests at `src` on b->stream (used both for capture
 // and for the direct path).
 static int enqueue_batch(nvshmemx_batch *b, bool with_events, const nvshmemx_request *src) {
-  if (b->cfg.stream) return enqueue_stream(b, with_events, src, nullptr, 0);
+  if (b->cfg.stream) return enqueue_stream(b, with_events, src);
   cudaMemsetAsync(b->d_ctl, 0, sizeof(BatchCtl), b->stream);
   return enqueue_piece(b, with_events, src, b->n, b->d_ctl, b->d_ctl, nullptr, 0, b->stream);
 }
@@ -1070,21 +952,12 @@ int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n
   if (!b || n < 0 || n > b->max_n || (n && !reqs)) return fail(NVSHMEMX_ERR_INVALID, "batch_submit: bad arguments");
   int rc;
   b->n = n;
-  const bool staged = b->cfg.stream && n > 0;
-  const int n0 = staged ? 0 : split_point(n);
-  if (!staged && !n0 && (rc = ensure_graph(b, b->d_reqs))) return rc;
+  const int n0 = b->cfg.stream ? 0 : split_point(n);
+  if (!n0 && (rc = ensure_graph(b, b->d_reqs))) return rc;
   b->last_split = n0 > 0;
   b->timed_direct = false;
   cudaEventRecord(b->ev_start, b->stream);
-  if (staged) {
-    // stream mode: the kernel starts at once and plans each piece of the
-    // requests as the copy stream lands it
-    if ((rc = enqueue_stream(b, false, b->d_reqs, reqs, n))) {
-      cudaStreamSynchronize(b->copy_stream);
-      cudaStreamSynchronize(b->stream);
-      return rc;
-    }
-  } else if (n0) {
+  if (n0) {
     // Two pieces: the first quarter is copied, planned and executed while
     // the copy stream brings the rest; the second piece is planned (its
     // items appended after the first's) and executed once both are done.

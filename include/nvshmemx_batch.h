@@ -91,12 +91,9 @@ int nvshmemx_batch_execute(nvshmemx_batch *b, int reps, float *out_ms);
  * whole 256-request blocks) is copied, planned and executed while a second
  * stream copies the rest, which is then planned and executed.  An invalid
  * request in the second piece is reported after the first piece has run
- * (with one piece, nothing runs).  In
- * stream mode the streaming kernel is launched first and the requests are
- * copied in growing pieces (2048, 4096, ... requests) on a second stream,
- * each piece followed by a stream write of the resident count that the
- * kernel's planners wait for, so the copy overlaps execution.  The requests
- * stay resident: nvshmemx_batch_execute afterwards runs the same batch. */
+ * (with one piece, nothing runs).  In stream mode the copy precedes the
+ * streaming kernel.  The requests stay resident: nvshmemx_batch_execute
+ * afterwards runs the same batch. */
 int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n, int *out_status,
                           float *out_ms);
 

@@ -147,12 +147,11 @@ def test_submit_pipelined_two_pieces(shmem_factory, cfg):
     sh.status()
 
 
-def test_stream_submit_staged_pieces(shmem_factory):
-    """End-to-end in stream mode: the streaming kernel starts at once and
-    plans each piece of the requests as the copy stream lands it (8192,
-    16384, 32768, ... requests per piece).  Batches of several sizes in a row
-    (three pieces, two, one) through the pinned buffer and from ordinary
-    (pageable) host memory."""
+def test_stream_submit(shmem_factory):
+    """End-to-end in stream mode (copy, then the streaming kernel): batches of
+    several sizes in a row through the pinned buffer and from ordinary
+    (pageable) host memory, then graph-mode and stream-mode executions of the
+    resident requests on the same object."""
     npes, heap = 16, 16 << 20
     sh, om = setup(shmem_factory, npes, heap)
     with sh.batch(30000, 256 << 20, 4096) as b:
@@ -168,7 +167,7 @@ def test_stream_submit_staged_pieces(shmem_factory):
             assert st == 0 and ms > 0
             om.apply_requests(reqs)
             assert first_diff(heap_images(sh, npes, heap), om.heap) is None, (seed, n)
-        # the staged requests stay resident: device-resident execution (the
+        # the submitted requests stay resident: device-resident execution (the
         # graph of the streaming kernel) of the last batch
         b.execute(2)
         om.apply_requests(reqs)
@@ -183,7 +182,7 @@ def test_stream_submit_staged_pieces(shmem_factory):
         om.apply_requests(reqs)
         om.apply_requests(reqs)
         assert first_diff(heap_images(sh, npes, heap), om.heap) is None
-        # an empty staged submit does nothing
+        # an empty submit does nothing
         st, _ = b.submit(buf, 0)
         assert st == 0
     assert sh.status() == 0
