@@ -45,6 +45,17 @@ __device__ __forceinline__ void set_status(BatchCtl *ctl, int code, int req) {
   if (atomicCAS(&ctl->status, 0, code) == 0) ctl->bad_request = req;
 }
 
+// Programmatic dependent launch: the plan kernel lets the exec kernel start
+// as soon as every plan CTA is running; the exec kernel sets up its rings,
+// then waits until the plan grid has completed and its writes are visible.
+// Both are no-ops for a launch without the programmatic attribute.
+__device__ __forceinline__ void pdl_release_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait_prerequisites() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // ------------------------------------------------------------------- plan
 // A batch is planned as one piece, or (pipelined submit) as consecutive
 // pieces: piece p appends its items after those of piece p-1 (`prev`, planned
@@ -56,6 +67,7 @@ __global__ void __launch_bounds__(256) batch_plan_kernel(Cfg c, const nvshmemx_r
                                                          const BatchCtl *prev, int req_base) {
   __shared__ unsigned warp_sums[8];
   __shared__ unsigned long long block_base;
+  pdl_release_dependents();
   const unsigned long long ibase = prev ? prev->item_base + prev->total_chunks : 0ull;
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->item_base = ibase;
   const int i = blockIdx.x * 256 + threadIdx.x;
@@ -145,9 +157,11 @@ __global__ void __launch_bounds__(256) batch_plan_kernel(Cfg c, const nvshmemx_r
 }
 
 // ------------------------------------------------------------------- exec
+// Items are read through L2 (the exec kernel may start before the plan
+// kernel that writes them has finished; see pdl_wait_prerequisites).
 __device__ __forceinline__ WorkItem load_item(const WorkItem *p) {
   const uint4 *q = reinterpret_cast<const uint4 *>(p);
-  uint4 a = __ldg(q), b = __ldg(q + 1);
+  uint4 a = __ldcg(q), b = __ldcg(q + 1);
   WorkItem w;
   w.dst = ((unsigned long long)a.y << 32) | a.x;
   w.src = ((unsigned long long)a.w << 32) | a.z;
@@ -180,6 +194,7 @@ template <int VB, int U>
 __global__ void __launch_bounds__(1024) batch_exec_kernel(const WorkItem *__restrict__ items, BatchCtl *ctl,
                                                           const BatchCtl *sctl, unsigned long long cap, int grab) {
   const unsigned lane = threadIdx.x & 31u;
+  pdl_wait_prerequisites();
   if (*(volatile const int *)&sctl->status != 0) return;
   unsigned long long C = *(volatile unsigned long long *)&ctl->total_chunks;
   const unsigned long long ib = *(volatile unsigned long long *)&ctl->item_base;
@@ -317,13 +332,13 @@ __global__ void __launch_bounds__(256) batch_exec_tma_kernel(const WorkItem *__r
                                                               unsigned SB, unsigned min_bulk, long long timeout_ns) {
   extern __shared__ __align__(128) char smem[];
   const unsigned lane = threadIdx.x & 31u;
-  if (*(volatile int *)&sctl->status != 0) return;
-  const unsigned long long C = *(volatile unsigned long long *)&ctl->total_chunks;
-  const unsigned long long ib = *(volatile unsigned long long *)&ctl->item_base;
-  if (ib + C > cap) return;
-  items += ib;
   WarpTma<S> ring;
-  ring.init(smem, SB, min_bulk, timeout_ns, lane);
+  ring.init(smem, SB, min_bulk, timeout_ns, lane);  // overlaps the plan kernel
+  pdl_wait_prerequisites();
+  unsigned long long C = *(volatile unsigned long long *)&ctl->total_chunks;
+  const unsigned long long ib = *(volatile unsigned long long *)&ctl->item_base;
+  if (*(volatile int *)&sctl->status != 0 || ib + C > cap) C = 0;  // nothing to run
+  items += ib;
   unsigned long long bse = 0;
   if (lane == 0) bse = atomicAdd(&ctl->cursor, (unsigned long long)grab);
   bse = __shfl_sync(0xffffffffu, bse, 0);
@@ -778,13 +793,26 @@ static int enqueue_piece(nvshmemx_batch *b, bool with_events, const nvshmemx_req
     batch_plan_kernel<<<(n + 255) / 256, 256, 0, st>>>(c, src, n, (unsigned)k.chunk_bytes, b->d_items, b->cap, ctl,
                                                        sctl, prev, req_base);
   if (with_events) cudaEventRecord(b->ev_exec0, st);
+  // Right after the plan kernel (no event between them), the exec kernel is
+  // a programmatic dependent launch: its set-up overlaps the plan's tail.
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(r.sm_count * ctas);
+  lc.blockDim = dim3(k.threads);
+  lc.dynamicSmemBytes = smem;
+  lc.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = attr;
+  lc.numAttrs = (n > 0 && !with_events) ? 1 : 0;
+  cudaError_t e;
   if (tfn)
-    tfn<<<r.sm_count * ctas, k.threads, smem, st>>>(b->d_items, ctl, sctl, b->cap, k.grab,
-                                                      (unsigned)k.tma_stage_bytes, (unsigned)k.tma_min_bytes,
-                                                      c.wait_timeout_ns);
+    e = cudaLaunchKernelEx(&lc, tfn, (const WorkItem *)b->d_items, ctl, sctl, b->cap, k.grab,
+                           (unsigned)k.tma_stage_bytes, (unsigned)k.tma_min_bytes, (long long)c.wait_timeout_ns);
   else
-    fn<<<r.sm_count * ctas, k.threads, 0, st>>>(b->d_items, ctl, sctl, b->cap, k.grab);
+    e = cudaLaunchKernelEx(&lc, fn, (const WorkItem *)b->d_items, ctl, (const BatchCtl *)sctl, b->cap, k.grab);
   if (with_events) cudaEventRecord(b->ev_exec1, st);
+  if (e != cudaSuccess) return check_cuda(e, "batch exec launch");
   return check_cuda(cudaGetLastError(), "batch launch");
 }
 
