@@ -252,7 +252,7 @@ def run_c1_sweep():
     return out
 
 
-def run_c2_sweep(peak):
+def run_c2_sweep(peak, only_size=0):
     """C2 all-to-all on 8 PEs across message sizes and element types: each
     round every PE puts (or gets) one message to (from) each of the 7 others,
     then quiet + device barrier; buffer sets rotate so large working sets
@@ -261,6 +261,8 @@ def run_c2_sweep(peak):
     out = {}
     plan = [(8, DT_INT), (512, DT_FLOAT), (32 << 10, DT_DOUBLE), (1 << 20, DT_FLOAT), (16 << 20, DT_INT),
             (256 << 20, DT_DOUBLE)]
+    if only_size:
+        plan = [(b, d) for b, d in plan if b == only_size] or [(only_size, DT_FLOAT)]
     for nbytes, dt in plan:
         nsets = max(1, min(8, (512 << 20) // (2 * 8 * 8 * nbytes)))
         heap = 2 * 8 * nbytes * nsets
@@ -285,12 +287,12 @@ def run_c2_sweep(peak):
     return out
 
 
-def run_c3_halo(peak):
+def run_c3_halo(peak, iters=100):
     """C3: 8 PEs on a periodic 2x2x2 grid, 256^3 float64 per PE, 100
     iterations of 6 face puts (x faces gathered with stride 256) + int_p
     signals + int_wait + device barrier."""
     from nvshmem_b200 import Shmem
-    n, iters = 256, 100
+    n = 256
     block, ghosts = n ** 3 * 8, 6 * n * n * 8
     heap = block + ghosts + 4096
     with Shmem(8, heap) as sh:
@@ -462,13 +464,25 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="c4", choices=["c4", "c4-small"])
-    ap.add_argument("--only", default="all", choices=["all", "batch"])
+    ap.add_argument("--only", default="all", choices=["all", "batch", "c2", "c3"],
+                    help="all: the contract line with every section; batch: the C4 line alone; "
+                         "c2 / c3: one diagnostic JSON line for that section alone (for profiling)")
+    ap.add_argument("--c2-size", type=int, default=0, help="with --only c2: one message size in bytes")
+    ap.add_argument("--c3-iters", type=int, default=100, help="with --only c3: timed iterations")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.only in ("c2", "c3"):
+        import torch
+        torch.cuda.set_device(local)
+        peak, _ = measured_peak()
+        out = run_c2_sweep(peak, args.c2_size) if args.only == "c2" else run_c3_halo(peak, args.c3_iters)
+        if rank == 0:
+            print(json.dumps({"section": args.only, "result": out}), flush=True)
         return
     run_gpu(args, rank, world, local)
 

@@ -356,18 +356,16 @@ __global__ void __launch_bounds__(256) batch_exec_tma_kernel(const WorkItem *__r
 
 // ------------------------------------------------ streaming: one launch
 // Planning and execution in one persistent cooperative launch.  The first
-// `planners` warps of every CTA read the requests -- from device memory, or
-// straight from pinned host memory for the end-to-end call, so the transfer
-// over the host link overlaps execution -- validate and translate them 32 at
-// a time, reserve their chunks with one atomicAdd per 32 requests on
-// ctl->total_chunks and publish each work item with a release store of the
-// launch's generation number in its last word.  Every warp (planners too,
-// once their share is planned) claims chunk indices from ctl->cursor and
-// waits for the item's generation tag before running it through its TMA
-// ring.  A warp stops at the first index at or beyond the final chunk count,
-// which is known once every planner has added itself to ctl->plan_done.
-// Unlike the graph path, an invalid request is skipped on its own (and
-// reported); the valid ones still run.
+// `planners` warps of every CTA claim groups of 32 requests in request order
+// (ctl->plan_cursor), validate and translate them, reserve their chunks with
+// one atomicAdd per group on ctl->total_chunks, write the work items and,
+// after one fence per group, tag each item with the launch's generation
+// number in its last word.  Every warp (planners too, once no group is left)
+// claims chunk indices from ctl->cursor and waits for the item's tag before
+// running it through its TMA ring; once a warp has seen every planner done
+// (ctl->plan_done) it knows the final chunk count and checks no more tags.
+// All waits are bounded.  Unlike the graph path, an invalid request is
+// skipped on its own (and reported); the valid ones still run.
 struct StreamCtl {                 // the first 32 bytes match BatchCtl
   unsigned long long total_chunks;
   unsigned long long cursor;
