@@ -325,6 +325,24 @@ static int init_impl(int npes, size_t heap) {
     release_all();
     return rc;
   }
+  // NVSHMEM_ENABLE_TRACING (nvshmem.cu:611-615) turns tracing on at start;
+  // NVSHMEM_LOG_BUFFER_SIZE keeps its unit, bytes (nvshmem.cu:145,618-622),
+  // here of trace ring per PE (48-byte records, rounded up to a power of two;
+  // default 2 MiB).  The processed trace files are written at stop.
+  const char *tv = getenv("NVSHMEM_ENABLE_TRACING");
+  if (tv && atol(tv) != 0) {
+    long long bytes = 2ll << 20;
+    const char *sv = getenv("NVSHMEM_LOG_BUFFER_SIZE");
+    if (sv && atoll(sv) > 0) bytes = atoll(sv);
+    long long recs = bytes / (long long)sizeof(nvshmemx_trace_record);
+    if (recs < 16) recs = 16;
+    if (recs > (1ll << 24)) recs = 1ll << 24;
+    if ((rc = nvshmemx_trace_enable((unsigned)recs))) {
+      release_all();
+      return rc;
+    }
+    r.trace_from_env = true;
+  }
   return NVSHMEMX_SUCCESS;
 }
 
@@ -391,6 +409,12 @@ int nvshmemx_finalize(void) {
   std::lock_guard<std::recursive_mutex> lk(r.mu);
   if (!r.started) return fail(NVSHMEMX_ERR_STATE, "nvstop_pes: not started");
   int rc = check_cuda(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+  if (r.trace_from_env && r.d_trace && rc == 0) {
+    // nvshmem_processed_tracefile_<pid>_<pe>, as the prototype's stop wrote
+    // (nvshmem.cu:377)
+    rc = nvshmemx_trace_write_csv(nullptr);
+  }
+  r.trace_from_env = false;
   release_all();
   return rc;
 }

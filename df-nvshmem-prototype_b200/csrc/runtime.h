@@ -43,6 +43,7 @@ struct Runtime {
   nvshmemx_trace_record *d_trace = nullptr;
   unsigned long long *d_trace_head = nullptr;
   unsigned trace_cap = 0;
+  bool trace_from_env = false;  // NVSHMEM_ENABLE_TRACING: write the CSV files at stop
   Cfg cfg{};
   // SPMD host threads
   bool spmd_active = false;

@@ -55,6 +55,41 @@ def test_trace_ring_records_and_csv(shmem_factory, tmp_path):
 CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p)
 
 
+def test_trace_from_environment(tmp_path):
+    """NVSHMEM_ENABLE_TRACING=1 at nvstart_pes turns the ring on (sized by
+    NVSHMEM_LOG_BUFFER_SIZE bytes per PE) and nvstop_pes writes one processed
+    trace file per PE, named as the prototype named them."""
+    import subprocess
+    import sys
+    pkg = os.path.dirname(os.path.dirname(L.__file__))
+    code = "\n".join([
+        "import os, sys",
+        f"sys.path.insert(0, {pkg!r})",
+        "from nvshmem_b200 import Shmem",
+        "from nvshmem_b200 import _lib as L",
+        "L.lib.nvstart_pes()",
+        "sh = Shmem.__new__(Shmem)",
+        "sh.npes, sh.heap_bytes = 2, 1 << 20",
+        "sh.base = L.lib.nvshmemx_arena_base()",
+        "flag = sh.alloc(4); data = sh.alloc(1024)",
+        "sh.pingpong(flag, data, 64, 20, skip=0)",
+        "assert L.lib.nvshmemx_status() == 0",
+        "L.lib.nvstop_pes()",
+        "print(os.getpid())",
+    ])
+    env = dict(os.environ, NVSHMEM_ENABLE_TRACING="1", NVSHMEM_LOG_BUFFER_SIZE=str(48 * 1024),
+               NVSHMEM_NPES="2", NVSHMEM_HEAP_SIZE=str(1 << 20), NVSHMEM_ERROR_MODE="return")
+    out = subprocess.run([sys.executable, "-c", code], cwd=tmp_path, env=env, capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr
+    pid = out.stdout.strip().splitlines()[-1]
+    for pe in range(2):
+        lines = (tmp_path / f"nvshmem_processed_tracefile_{pid}_{pe}").read_text().splitlines()
+        assert lines[0].startswith("# timestamp, gridid, blockid, tid, type")
+        ops = [ln.split(", ")[4] for ln in lines[1:]]
+        assert ops.count("wait_int") == 20
+
+
 def test_spmd_threads(shmem_factory):
     npes = 4
     sh = shmem_factory(npes, 1 << 20)
