@@ -100,3 +100,43 @@ def test_signal_values(shmem_factory):
     om.apply_requests(reqs)
     assert sh.status() == 0
     assert first_diff(heap_images(sh, 3, HEAP), om.heap) is None
+
+
+def test_direct_loads_and_stores_through_nvshmem_ptr(tmp_path):
+    """A CUDA application compiled against libnvshmem.a dereferences the
+    addresses nvshmem_ptr (host) and nvshmemx_ptr (device) return: plain
+    stores into the next PE's slice, quiet + device barrier, plain loads from
+    the previous PE's slice, then ordinary launches copying between slices
+    through host-side nvshmem_ptr pointers (tests/native/ptr_direct.cu).  The
+    heap images must equal the oracle's for the same puts and gets."""
+    import os
+    import subprocess
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = tmp_path / "ptr_direct"
+    r = subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-rdc=true",
+                        "-I", os.path.join(repo, "include"), os.path.join(repo, "tests", "native", "ptr_direct.cu"),
+                        "-o", str(exe), "-L", os.path.join(repo, "df-nvshmem-prototype_b200", "lib"), "-lnvshmem",
+                        "-L/usr/local/cuda/lib64/stubs", "-lcuda"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+    npes, heap = 4, 1 << 20
+    env = dict(os.environ, NVSHMEM_NPES=str(npes), NVSHMEM_HEAP_SIZE=str(heap))
+    out = tmp_path / "heaps.bin"
+    r = subprocess.run([str(exe), str(out)], capture_output=True, text=True, env=env, timeout=300)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    send, recv, got, copy2, n, np_, heap_ = map(int, r.stdout.split())
+    assert (np_, heap_) == (npes, heap)
+    images = np.fromfile(out, dtype=np.uint8).reshape(npes, heap)
+    om = Model(npes, heap)
+    i = np.arange(heap, dtype=np.int64)
+    for pe in range(npes):
+        om.heap[pe][:] = ((pe * 131 + i * 7 + (i >> 8)) & 0xff).astype(np.uint8)
+    ring = [dict(src_off=send, dst_off=recv, bytes=n, src_pe=p, dst_pe=(p + 1) % npes, op=REQ_PUT, dtype=DT_INT)
+            for p in range(npes)]
+    pull = [dict(src_off=send, dst_off=got, bytes=n, src_pe=(p - 1) % npes, dst_pe=p, op=REQ_GET, dtype=DT_INT)
+            for p in range(npes)]
+    host = [dict(src_off=recv, dst_off=copy2, bytes=n, src_pe=(q + 1) % npes, dst_pe=q, op=REQ_PUT, dtype=DT_INT)
+            for q in range(npes)]
+    for batch in (ring, pull, host):
+        om.apply_requests(requests(batch))
+    assert first_diff(images, om.heap) is None
+    assert not np.array_equal(images[0, recv:recv + n], images[0, send:send + n])  # the exchange moved data
