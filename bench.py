@@ -290,7 +290,9 @@ def run_c2_sweep(peak, only_size=0):
 def run_c3_halo(peak, iters=100):
     """C3: 8 PEs on a periodic 2x2x2 grid, 256^3 float64 per PE, 100
     iterations of 6 face puts (x faces gathered with stride 256) + int_p
-    signals + int_wait + device barrier."""
+    signals + int_wait + a barrier: the device barrier inside one persistent
+    launch (headline), and one launch per iteration followed by
+    nvshmem_barrier_all_offload (the prototype's structure)."""
     from nvshmem_b200 import Shmem
     n = 256
     block, ghosts = n ** 3 * 8, 6 * n * n * 8
@@ -305,10 +307,14 @@ def run_c3_halo(peak, iters=100):
         for pe in range(8):
             sh.memset(pe, block + ghosts, 0, 64)
         ms = sh.halo(2, 2, 2, n, 0, block, block + ghosts, iters, 74)
+        for pe in range(8):
+            sh.memset(pe, block + ghosts, 0, 64)
+        ms_off = sh.halo(2, 2, 2, n, 0, block, block + ghosts, iters, 74, offload=True)
         assert sh.status() == 0
     face_bytes = 8 * 6 * n * n * 8
     return {"us_per_iter": round(1e3 * ms / iters, 2), "face_GBps": round(2 * face_bytes * iters / (ms / 1e3) / 1e9, 1),
-            "iters": iters, "n": n, "ctas_per_pe": 74}
+            "iters": iters, "n": n, "ctas_per_pe": 74,
+            "offload_barrier_us_per_iter": round(1e3 * ms_off / iters, 2)}
 
 
 def run_c5_picker():

@@ -359,8 +359,13 @@ __device__ __forceinline__ int halo_nbr(int pe, int d, int px, int py, int pz) {
   return x + px * (y + py * z);
 }
 
+// `iters` iterations numbered from it0 (signal values it0 + it + 1); with
+// device_barrier each iteration ends at the device barrier, without it the
+// caller follows the launch with nvshmem_barrier_all_offload (one iteration
+// per launch, the prototype's own structure).
 __global__ void halo_kernel(Cfg c, int px, int py, int pz, int n, unsigned long long block_off,
-                            unsigned long long ghost_off, unsigned long long sig_off, int iters) {
+                            unsigned long long ghost_off, unsigned long long sig_off, int iters, int it0,
+                            int device_barrier) {
   const int pe = blockIdx.z;
   const unsigned lane = threadIdx.x & 31u;
   const unsigned long long face_bytes = (unsigned long long)n * n * 8ull;
@@ -394,10 +399,10 @@ __global__ void halo_kernel(Cfg c, int px, int py, int pz, int n, unsigned long 
     if (blockIdx.x == 0 && threadIdx.x < 6) {
       const int d = threadIdx.x;
       nvshmem_quiet();
-      nvshmem_int_p((int *)(c.arena + sig_off) + (d ^ 1), it + 1, halo_nbr(pe, d, px, py, pz));
-      nvshmem_int_wait_until(my_sig + d, 0, it + 1);
+      nvshmem_int_p((int *)(c.arena + sig_off) + (d ^ 1), it0 + it + 1, halo_nbr(pe, d, px, py, pz));
+      nvshmem_int_wait_until(my_sig + d, 0, it0 + it + 1);
     }
-    nvshmemx_barrier_all_ep((unsigned long long)it);
+    if (device_barrier) nvshmemx_barrier_all_ep((unsigned long long)it);
   }
 }
 
@@ -642,8 +647,8 @@ int nvshmemx_op_alltoall(int op, int dtype, size_t send_off, size_t recv_off, si
   return check_cuda(cudaDeviceSynchronize(), "alltoall");
 }
 
-int nvshmemx_op_halo(int px, int py, int pz, int n, size_t block_off, size_t ghost_off, size_t sig_off, int iters,
-                     int ctas_per_pe, float *out_ms) {
+static int halo_check(int px, int py, int pz, int n, size_t block_off, size_t ghost_off, size_t sig_off, int iters,
+                      int ctas_per_pe) {
   int rc;
   if ((rc = need_started())) return rc;
   const Runtime &r = rt();
@@ -653,9 +658,17 @@ int nvshmemx_op_halo(int px, int py, int pz, int n, size_t block_off, size_t gho
   if (block_off + nn * nn * nn * 8 > r.heap_bytes || ghost_off + 6 * nn * nn * 8 > r.heap_bytes ||
       sig_off + 24 > r.heap_bytes || (block_off | ghost_off) % 16 || sig_off % 4)
     return fail(NVSHMEMX_ERR_INVALID, "halo: buffers exceed the heap or are misaligned");
-  Cfg c = r.cfg;
+  return 0;
+}
+
+int nvshmemx_op_halo(int px, int py, int pz, int n, size_t block_off, size_t ghost_off, size_t sig_off, int iters,
+                     int ctas_per_pe, float *out_ms) {
+  int rc;
+  if ((rc = halo_check(px, py, pz, n, block_off, ghost_off, sig_off, iters, ctas_per_pe))) return rc;
+  Cfg c = rt().cfg;
   unsigned long long bo = block_off, go = ghost_off, so = sig_off;
-  void *args[] = {&c, &px, &py, &pz, &n, &bo, &go, &so, &iters};
+  int it0 = 0, device_barrier = 1;
+  void *args[] = {&c, &px, &py, &pz, &n, &bo, &go, &so, &iters, &it0, &device_barrier};
   EventTimer t;
   t.start();
   if ((rc = launch_collective((const void *)halo_kernel, dim3(ctas_per_pe), dim3(256), args, 0, 0))) return rc;
@@ -663,6 +676,27 @@ int nvshmemx_op_halo(int px, int py, int pz, int n, size_t block_off, size_t gho
   float ms = t.ms();
   if (out_ms) *out_ms = ms;
   return check_cuda(cudaDeviceSynchronize(), "halo");
+}
+
+int nvshmemx_op_halo_offload(int px, int py, int pz, int n, size_t block_off, size_t ghost_off, size_t sig_off,
+                             int iters, int ctas_per_pe, float *out_ms) {
+  int rc;
+  if ((rc = halo_check(px, py, pz, n, block_off, ghost_off, sig_off, iters, ctas_per_pe))) return rc;
+  Cfg c = rt().cfg;
+  unsigned long long bo = block_off, go = ghost_off, so = sig_off;
+  int one = 1, device_barrier = 0;
+  EventTimer t;
+  t.start();
+  for (int it = 0; it < iters; ++it) {
+    void *args[] = {&c, &px, &py, &pz, &n, &bo, &go, &so, &one, &it, &device_barrier};
+    if ((rc = launch_collective((const void *)halo_kernel, dim3(ctas_per_pe), dim3(256), args, 0, 0))) return rc;
+    nvshmem_barrier_all_offload();
+    if ((rc = last_launch("halo_offload barrier"))) return rc;
+  }
+  t.stop();
+  float ms = t.ms();
+  if (out_ms) *out_ms = ms;
+  return check_cuda(cudaDeviceSynchronize(), "halo_offload");
 }
 
 int nvshmemx_op_wait_test(size_t flag_off, int value, long long timeout_ns, int *out_status) {

@@ -126,10 +126,12 @@ class Shmem:
                                        set_stride, mode, ctas_per_pe, byref(ms)), "alltoall")
         return ms.value
 
-    def halo(self, px, py, pz, n, block_off, ghost_off, sig_off, iters, ctas_per_pe) -> float:
+    def halo(self, px, py, pz, n, block_off, ghost_off, sig_off, iters, ctas_per_pe, offload=False) -> float:
+        """C3 exchange; offload=True runs one launch per iteration followed by
+        nvshmem_barrier_all_offload, as the prototype structures it."""
         ms = c_float(0)
-        check(lib.nvshmemx_op_halo(px, py, pz, n, block_off, ghost_off, sig_off, iters,
-                                   ctas_per_pe, byref(ms)), "halo")
+        fn = lib.nvshmemx_op_halo_offload if offload else lib.nvshmemx_op_halo
+        check(fn(px, py, pz, n, block_off, ghost_off, sig_off, iters, ctas_per_pe, byref(ms)), "halo")
         return ms.value
 
     def wait_test(self, flag_off, value, timeout_ns) -> int:

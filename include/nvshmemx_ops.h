@@ -121,6 +121,11 @@ int nvshmemx_op_alltoall(int op, int dtype, size_t send_off, size_t recv_off, si
  * and meets the others at the device barrier. */
 int nvshmemx_op_halo(int px, int py, int pz, int n, size_t block_off, size_t ghost_off,
                      size_t sig_off, int iters, int ctas_per_pe, float *out_ms);
+/* The same exchange in the prototype's own structure: one collective launch
+ * per iteration (faces, quiet, signals, waits) followed by the host's
+ * nvshmem_barrier_all_offload(), iters times; the heaps end identical. */
+int nvshmemx_op_halo_offload(int px, int py, int pz, int n, size_t block_off, size_t ghost_off,
+                             size_t sig_off, int iters, int ctas_per_pe, float *out_ms);
 
 /* ---- failure detection ---------------------------------------------------
  * One thread of PE 0 waits (nvshmemx_int_wait_until_cmp EQ) on the int at

@@ -107,8 +107,9 @@ def test_alltoall_large_on_device_compare(shmem_factory):
             assert sh.compare(q, npes * nbytes + p * nbytes, p, q * nbytes, nbytes) == 0
 
 
+@pytest.mark.parametrize("offload", [False, True], ids=["persistent", "offload_barrier"])
 @pytest.mark.parametrize("n", [8, 32])
-def test_halo_bit_exact(shmem_factory, n):
+def test_halo_bit_exact(shmem_factory, n, offload):
     npes = 8
     block = n * n * n * 8
     heap = block + 6 * n * n * 8 + 4096
@@ -120,7 +121,7 @@ def test_halo_bit_exact(shmem_factory, n):
         b = c3_block(n, pe)
         sh.write(pe, block_off, b)
         om.heap[pe, block_off:block_off + block] = b.view(np.uint8)
-    sh.halo(2, 2, 2, n, block_off, ghost_off, sig_off, iters=5, ctas_per_pe=4)
+    sh.halo(2, 2, 2, n, block_off, ghost_off, sig_off, iters=5, ctas_per_pe=4, offload=offload)
     assert sh.status() == 0
     om.halo(2, 2, 2, n, block_off, ghost_off, sig_off, 5)
     assert first_diff(heap_images(sh, npes, heap), om.heap) is None
