@@ -278,6 +278,14 @@ def run_c2_sweep(peak, only_size=0):
                 ms = sh.alltoall(op, dt, 0, 8 * nbytes, nbytes, **kw)
                 gbs = 2 * 8 * 7 * nbytes * rounds / (ms / 1e3) / 1e9
                 row[name] = {"GBps": round(gbs, 1), "frac": round(gbs / peak, 3), "us_per_round": round(1e3 * ms / rounds, 2)}
+            # the prototype's structure: a launch per round, then the host's
+            # nvshmem_barrier_all (device synchronisation + host barrier)
+            kw = dict(rounds=min(rounds, 50), nsets=nsets, set_stride=16 * nbytes, mode=MODE_BULK, ctas_per_pe=18,
+                      host_rounds=True)
+            ms = sh.alltoall(REQ_PUT, dt, 0, 8 * nbytes, nbytes, **kw)
+            gbs = 2 * 8 * 7 * nbytes * kw["rounds"] / (ms / 1e3) / 1e9
+            row["put_host_rounds"] = {"GBps": round(gbs, 1), "frac": round(gbs / peak, 3),
+                                      "us_per_round": round(1e3 * ms / kw["rounds"], 2)}
             for p in range(8):
                 for q in range(8):
                     if p != q:

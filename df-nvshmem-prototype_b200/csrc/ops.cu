@@ -277,7 +277,7 @@ __global__ void barrier_latency_kernel(int iters, int counted, long long *cycles
 template <int MODE>
 __global__ void alltoall_kernel(Cfg c, int op, int dtype, unsigned long long send_off,
                                 unsigned long long recv_off, unsigned long long bytes, int rounds, int nsets,
-                                unsigned long long set_stride, unsigned bulk_smem) {
+                                unsigned long long set_stride, unsigned bulk_smem, int device_barrier) {
   extern __shared__ __align__(128) char smem[];
   const int pe = blockIdx.z, np = c.npes;
   const unsigned long long total = (unsigned long long)(np - 1) * bytes;
@@ -342,7 +342,7 @@ __global__ void alltoall_kernel(Cfg c, int op, int dtype, unsigned long long sen
     // stores before the leader, whose quiet and release cover them all
     __syncthreads();
     if (threadIdx.x == 0) nvshmem_quiet();
-    nvshmemx_barrier_all_ep((unsigned long long)r);
+    if (device_barrier) nvshmemx_barrier_all_ep((unsigned long long)r);
   }
 }
 
@@ -606,8 +606,11 @@ int nvshmemx_op_offload_barrier(int iters, double *out_us_per_call) {
   return check_cuda(cudaDeviceSynchronize(), "offload barrier");
 }
 
-int nvshmemx_op_alltoall(int op, int dtype, size_t send_off, size_t recv_off, size_t bytes, int rounds, int nsets,
-                         size_t set_stride, int mode, int ctas_per_pe, float *out_ms) {
+// Validates the arguments and picks the kernel, grid and block of an
+// all-to-all in `mode`.
+static int alltoall_setup(int op, int dtype, size_t send_off, size_t recv_off, size_t bytes, int rounds, int nsets,
+                          size_t set_stride, int mode, int ctas_per_pe, const void **fn, dim3 *grid, dim3 *block,
+                          unsigned *smem) {
   int rc;
   if ((rc = need_started())) return rc;
   const Runtime &r = rt();
@@ -622,22 +625,35 @@ int nvshmemx_op_alltoall(int op, int dtype, size_t send_off, size_t recv_off, si
   const size_t last = (size_t)(nsets - 1) * set_stride;
   if (send_off + last + span > r.heap_bytes || recv_off + last + span > r.heap_bytes)
     return fail(NVSHMEMX_ERR_INVALID, "alltoall: buffers exceed the heap");
-  Cfg c = r.cfg;
-  unsigned long long so = send_off, ro = recv_off, by = bytes, ss = set_stride;
-  unsigned smem = mode == NVSHMEMX_MODE_BULK ? kBulkSmem : 0;
-  void *args[] = {&c, &op, &dtype, &so, &ro, &by, &rounds, &nsets, &ss, &smem};
-  const void *fn;
-  dim3 grid(ctas_per_pe), block(256);
+  *smem = mode == NVSHMEMX_MODE_BULK ? kBulkSmem : 0;
+  *grid = dim3(ctas_per_pe);
+  *block = dim3(256);
   switch (mode) {
     case NVSHMEMX_MODE_THREAD:
-      fn = (const void *)alltoall_kernel<NVSHMEMX_MODE_THREAD>;
-      grid = dim3(1);
-      block = dim3(32 * ((r.npes - 1 + 31) / 32));
+      *fn = (const void *)alltoall_kernel<NVSHMEMX_MODE_THREAD>;
+      *grid = dim3(1);
+      *block = dim3(32 * ((r.npes - 1 + 31) / 32));
       break;
-    case NVSHMEMX_MODE_WARP: fn = (const void *)alltoall_kernel<NVSHMEMX_MODE_WARP>; break;
-    case NVSHMEMX_MODE_BLOCK: fn = (const void *)alltoall_kernel<NVSHMEMX_MODE_BLOCK>; break;
-    default: fn = (const void *)alltoall_kernel<NVSHMEMX_MODE_BULK>;
+    case NVSHMEMX_MODE_WARP: *fn = (const void *)alltoall_kernel<NVSHMEMX_MODE_WARP>; break;
+    case NVSHMEMX_MODE_BLOCK: *fn = (const void *)alltoall_kernel<NVSHMEMX_MODE_BLOCK>; break;
+    default: *fn = (const void *)alltoall_kernel<NVSHMEMX_MODE_BULK>;
   }
+  return 0;
+}
+
+int nvshmemx_op_alltoall(int op, int dtype, size_t send_off, size_t recv_off, size_t bytes, int rounds, int nsets,
+                         size_t set_stride, int mode, int ctas_per_pe, float *out_ms) {
+  int rc;
+  const void *fn;
+  dim3 grid, block;
+  unsigned smem;
+  if ((rc = alltoall_setup(op, dtype, send_off, recv_off, bytes, rounds, nsets, set_stride, mode, ctas_per_pe, &fn,
+                           &grid, &block, &smem)))
+    return rc;
+  Cfg c = rt().cfg;
+  unsigned long long so = send_off, ro = recv_off, by = bytes, ss = set_stride;
+  int device_barrier = 1;
+  void *args[] = {&c, &op, &dtype, &so, &ro, &by, &rounds, &nsets, &ss, &smem, &device_barrier};
   EventTimer t;
   t.start();
   if ((rc = launch_collective(fn, grid, block, args, smem, 0))) return rc;
@@ -645,6 +661,34 @@ int nvshmemx_op_alltoall(int op, int dtype, size_t send_off, size_t recv_off, si
   float ms = t.ms();
   if (out_ms) *out_ms = ms;
   return check_cuda(cudaDeviceSynchronize(), "alltoall");
+}
+
+int nvshmemx_op_alltoall_host(int op, int dtype, size_t send_off, size_t recv_off, size_t bytes, int rounds,
+                              int nsets, size_t set_stride, int mode, int ctas_per_pe, float *out_ms) {
+  int rc;
+  const void *fn;
+  dim3 grid, block;
+  unsigned smem;
+  if ((rc = alltoall_setup(op, dtype, send_off, recv_off, bytes, rounds, nsets, set_stride, mode, ctas_per_pe, &fn,
+                           &grid, &block, &smem)))
+    return rc;
+  Cfg c = rt().cfg;
+  unsigned long long by = bytes, ss = 0;
+  int one = 1, device_barrier = 0;
+  EventTimer t;
+  t.start();
+  for (int rd = 0; rd < rounds; ++rd) {
+    unsigned long long so = send_off + (size_t)(rd % nsets) * set_stride;
+    unsigned long long ro = recv_off + (size_t)(rd % nsets) * set_stride;
+    void *args[] = {&c, &op, &dtype, &so, &ro, &by, &one, &one, &ss, &smem, &device_barrier};
+    if ((rc = launch_collective(fn, grid, block, args, smem, 0))) return rc;
+    nvshmem_barrier_all();
+    if ((rc = last_launch("alltoall_host round"))) return rc;
+  }
+  t.stop();
+  float ms = t.ms();
+  if (out_ms) *out_ms = ms;
+  return check_cuda(cudaDeviceSynchronize(), "alltoall_host");
 }
 
 static int halo_check(int px, int py, int pz, int n, size_t block_off, size_t ghost_off, size_t sig_off, int iters,

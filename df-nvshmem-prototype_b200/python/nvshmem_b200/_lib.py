@@ -113,6 +113,8 @@ _SIGS = {
     "nvshmemx_op_offload_barrier": (c_int, [c_int, _P(c_double)]),
     "nvshmemx_op_alltoall": (c_int, [c_int, c_int, c_size_t, c_size_t, c_size_t, c_int, c_int,
                                      c_size_t, c_int, c_int, _P(c_float)]),
+    "nvshmemx_op_alltoall_host": (c_int, [c_int, c_int, c_size_t, c_size_t, c_size_t, c_int, c_int,
+                                          c_size_t, c_int, c_int, _P(c_float)]),
     "nvshmemx_op_halo": (c_int, [c_int, c_int, c_int, c_int, c_size_t, c_size_t, c_size_t, c_int,
                                  c_int, _P(c_float)]),
     "nvshmemx_op_halo_offload": (c_int, [c_int, c_int, c_int, c_int, c_size_t, c_size_t, c_size_t, c_int,

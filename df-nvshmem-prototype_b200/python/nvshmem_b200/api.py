@@ -120,10 +120,13 @@ class Shmem:
         return us.value
 
     def alltoall(self, op, dtype, send_off, recv_off, nbytes, rounds=1, nsets=1, set_stride=0,
-                 mode=L.MODE_BLOCK, ctas_per_pe=1) -> float:
+                 mode=L.MODE_BLOCK, ctas_per_pe=1, host_rounds=False) -> float:
+        """C2 rounds; host_rounds=True runs one launch per round followed by the
+        host's nvshmem_barrier_all, as the prototype structures it."""
         ms = c_float(0)
-        check(lib.nvshmemx_op_alltoall(op, dtype, send_off, recv_off, nbytes, rounds, nsets,
-                                       set_stride, mode, ctas_per_pe, byref(ms)), "alltoall")
+        fn = lib.nvshmemx_op_alltoall_host if host_rounds else lib.nvshmemx_op_alltoall
+        check(fn(op, dtype, send_off, recv_off, nbytes, rounds, nsets, set_stride, mode, ctas_per_pe, byref(ms)),
+              "alltoall")
         return ms.value
 
     def halo(self, px, py, pz, n, block_off, ghost_off, sig_off, iters, ctas_per_pe, offload=False) -> float:

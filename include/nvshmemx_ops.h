@@ -109,6 +109,12 @@ int nvshmemx_op_offload_barrier(int iters, double *out_us_per_call);
 int nvshmemx_op_alltoall(int op, int dtype, size_t send_off, size_t recv_off, size_t bytes,
                          int rounds, int nsets, size_t set_stride, int mode, int ctas_per_pe,
                          float *out_ms);
+/* The same rounds in the prototype's own structure: one collective launch
+ * per round (puts or gets, then nvshmem_quiet) followed by the host's
+ * nvshmem_barrier_all(); the heaps end identical. */
+int nvshmemx_op_alltoall_host(int op, int dtype, size_t send_off, size_t recv_off, size_t bytes,
+                              int rounds, int nsets, size_t set_stride, int mode, int ctas_per_pe,
+                              float *out_ms);
 
 /* ---- C3: halo exchange on a periodic px x py x pz PE grid ----------------
  * Each PE owns an n^3 float64 block at block_off (x fastest).  Per iteration

@@ -75,7 +75,11 @@ def test_alltoall_small_sizes(shmem_factory, mode, op):
     assert first_diff(heap_images(sh, npes, heap), om.heap) is None
 
 
-def test_alltoall_rotating_sets(shmem_factory):
+@pytest.mark.parametrize("host_rounds", [False, True], ids=["device_barrier", "host_barrier"])
+def test_alltoall_rotating_sets(shmem_factory, host_rounds):
+    """Rounds over rotating buffer sets, in one launch with the device barrier
+    and in the prototype's structure (a launch per round, then the host's
+    nvshmem_barrier_all)."""
     npes, heap = 8, 8 << 20
     sh = shmem_factory(npes, heap)
     om = Model(npes, heap)
@@ -84,7 +88,7 @@ def test_alltoall_rotating_sets(shmem_factory):
         om.fill_random(pe, 0, heap, 9)
     nbytes, stride = 65536, 1 << 20
     sh.alltoall(REQ_PUT, DT_FLOAT, 0, 4 << 20, nbytes, rounds=5, nsets=3, set_stride=stride,
-                mode=MODE_BULK, ctas_per_pe=4)
+                mode=MODE_BULK, ctas_per_pe=4, host_rounds=host_rounds)
     om.alltoall(0, 0, 4 << 20, nbytes, rounds=5, nsets=3, set_stride=stride)
     assert sh.status() == 0
     assert first_diff(heap_images(sh, npes, heap), om.heap) is None
