@@ -19,46 +19,50 @@ using nvshm::Cfg;
 namespace {
 
 template <typename T>
-__device__ __forceinline__ void put_thread(T *target, const T *source, int len, int pe, int op) {
+__device__ __noinline__ void put_thread(T *target, const T *source, int len, int pe, int op) {
   const Cfg &c = CFG;
   const unsigned long long bytes = nvshm::elem_bytes<T>(len);
   if (!nvshm::check_remote(c, target, bytes, pe) || !nvshm::check_local(c, source, bytes)) return;
   char *dst = nvshm::xlate(c, target, pe);
   unsigned long long t0 = c.trace ? nvshm::gtimer() : 0;
-  nvshm::copy_coop<16, 4>(dst, reinterpret_cast<const char *>(source), bytes, 0, 1);
+  // one thread: 16 vector accesses in flight (measured 2.6x the bandwidth of 4
+  // for a 1 MiB put, 2.2x on a batch of calls, at 90 instead of 54 registers)
+  nvshm::copy_coop<16, 16>(dst, reinterpret_cast<const char *>(source), bytes, 0, 1);
   if (c.trace) nvshm::trace_rec(c, op, source, dst, bytes, pe, t0, nvshm::gtimer());
 }
 
 template <typename T>
-__device__ __forceinline__ void get_thread(T *target, const T *source, int len, int pe, int op) {
+__device__ __noinline__ void get_thread(T *target, const T *source, int len, int pe, int op) {
   const Cfg &c = CFG;
   const unsigned long long bytes = nvshm::elem_bytes<T>(len);
   if (!nvshm::check_remote(c, source, bytes, pe) || !nvshm::check_local(c, target, bytes)) return;
   const char *src = nvshm::xlate(c, source, pe);
   unsigned long long t0 = c.trace ? nvshm::gtimer() : 0;
-  nvshm::copy_coop<16, 4>(reinterpret_cast<char *>(target), src, bytes, 0, 1);
+  nvshm::copy_coop<16, 16>(reinterpret_cast<char *>(target), src, bytes, 0, 1);
   if (c.trace) nvshm::trace_rec(c, op, target, src, bytes, pe, t0, nvshm::gtimer());
 }
 
 // Cooperative forms: `r` of `n` threads; bounds are checked by every thread
 // (same arguments, same answer) so all skip together.
-__device__ __forceinline__ void putmem_coop(void *target, const void *source, unsigned long long bytes,
+__device__ __noinline__ void putmem_coop(void *target, const void *source, unsigned long long bytes,
                                             int pe, unsigned r, unsigned n, int op) {
   const Cfg &c = CFG;
   if (!nvshm::check_remote(c, target, bytes, pe) || !nvshm::check_local(c, source, bytes)) return;
   char *dst = nvshm::xlate(c, target, pe);
   unsigned long long t0 = (c.trace && r == 0) ? nvshm::gtimer() : 0;
-  nvshm::copy_coop<16, 4>(dst, reinterpret_cast<const char *>(source), bytes, r, n);
+  // 8 vector accesses in flight per thread (measured against 4 and 16: C2
+  // 16 MiB block / warp all-to-all 0.66 / 0.72 -> 0.81 / 0.91 of the copy peak)
+  nvshm::copy_coop<16, 8>(dst, reinterpret_cast<const char *>(source), bytes, r, n);
   if (c.trace && r == 0) nvshm::trace_rec(c, op, source, dst, bytes, pe, t0, nvshm::gtimer());
 }
 
-__device__ __forceinline__ void getmem_coop(void *target, const void *source, unsigned long long bytes,
+__device__ __noinline__ void getmem_coop(void *target, const void *source, unsigned long long bytes,
                                             int pe, unsigned r, unsigned n, int op) {
   const Cfg &c = CFG;
   if (!nvshm::check_remote(c, source, bytes, pe) || !nvshm::check_local(c, target, bytes)) return;
   const char *src = nvshm::xlate(c, source, pe);
   unsigned long long t0 = (c.trace && r == 0) ? nvshm::gtimer() : 0;
-  nvshm::copy_coop<16, 4>(reinterpret_cast<char *>(target), src, bytes, r, n);
+  nvshm::copy_coop<16, 8>(reinterpret_cast<char *>(target), src, bytes, r, n);
   if (c.trace && r == 0) nvshm::trace_rec(c, op, target, src, bytes, pe, t0, nvshm::gtimer());
 }
 

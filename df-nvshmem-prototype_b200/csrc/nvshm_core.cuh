@@ -185,6 +185,16 @@ __device__ __forceinline__ void copy_body(char *__restrict__ dst, const char *__
       for (int u = 0; u < U; ++u) d[i + (unsigned long long)u * nthr] = v[u];
     }
   }
+  // copies too short for U accesses per thread still get 4 in flight
+  if (U > 4) {
+    for (; i + 3ull * nthr < nv; i += 4ull * nthr) {
+      V v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = s[i + (unsigned long long)u * nthr];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) d[i + (unsigned long long)u * nthr] = v[u];
+    }
+  }
   for (; i < nv; i += nthr) d[i] = s[i];
   for (unsigned long long j = head + nv * VB + r; j < bytes; j += nthr) dst[j] = src[j];
 }

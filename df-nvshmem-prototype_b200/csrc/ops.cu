@@ -363,7 +363,7 @@ __device__ __forceinline__ int halo_nbr(int pe, int d, int px, int py, int pz) {
 // device_barrier each iteration ends at the device barrier, without it the
 // caller follows the launch with nvshmem_barrier_all_offload (one iteration
 // per launch, the prototype's own structure).
-__global__ void halo_kernel(Cfg c, int px, int py, int pz, int n, unsigned long long block_off,
+__global__ void __launch_bounds__(256, 4) halo_kernel(Cfg c, int px, int py, int pz, int n, unsigned long long block_off,
                             unsigned long long ghost_off, unsigned long long sig_off, int iters, int it0,
                             int device_barrier) {
   const int pe = blockIdx.z;
@@ -691,12 +691,15 @@ int nvshmemx_op_alltoall_host(int op, int dtype, size_t send_off, size_t recv_of
   return check_cuda(cudaDeviceSynchronize(), "alltoall_host");
 }
 
+// ctas_per_pe 0: as many CTAs per PE as stay co-resident (the exchange is
+// latency-bound, so more warps in flight help).
 static int halo_check(int px, int py, int pz, int n, size_t block_off, size_t ghost_off, size_t sig_off, int iters,
-                      int ctas_per_pe) {
+                      int *ctas_per_pe) {
   int rc;
   if ((rc = need_started())) return rc;
   const Runtime &r = rt();
-  if (px < 1 || py < 1 || pz < 1 || px * py * pz != r.npes || n < 1 || iters < 1 || ctas_per_pe < 1)
+  if (*ctas_per_pe == 0) *ctas_per_pe = max_ctas_per_pe((const void *)halo_kernel, 256, 0);
+  if (px < 1 || py < 1 || pz < 1 || px * py * pz != r.npes || n < 1 || iters < 1 || *ctas_per_pe < 1)
     return fail(NVSHMEMX_ERR_INVALID, "halo: grid %dx%dx%d does not match %d PEs", px, py, pz, r.npes);
   const size_t nn = (size_t)n;
   if (block_off + nn * nn * nn * 8 > r.heap_bytes || ghost_off + 6 * nn * nn * 8 > r.heap_bytes ||
@@ -708,7 +711,7 @@ static int halo_check(int px, int py, int pz, int n, size_t block_off, size_t gh
 int nvshmemx_op_halo(int px, int py, int pz, int n, size_t block_off, size_t ghost_off, size_t sig_off, int iters,
                      int ctas_per_pe, float *out_ms) {
   int rc;
-  if ((rc = halo_check(px, py, pz, n, block_off, ghost_off, sig_off, iters, ctas_per_pe))) return rc;
+  if ((rc = halo_check(px, py, pz, n, block_off, ghost_off, sig_off, iters, &ctas_per_pe))) return rc;
   Cfg c = rt().cfg;
   unsigned long long bo = block_off, go = ghost_off, so = sig_off;
   int it0 = 0, device_barrier = 1;
@@ -725,7 +728,7 @@ int nvshmemx_op_halo(int px, int py, int pz, int n, size_t block_off, size_t gho
 int nvshmemx_op_halo_offload(int px, int py, int pz, int n, size_t block_off, size_t ghost_off, size_t sig_off,
                              int iters, int ctas_per_pe, float *out_ms) {
   int rc;
-  if ((rc = halo_check(px, py, pz, n, block_off, ghost_off, sig_off, iters, ctas_per_pe))) return rc;
+  if ((rc = halo_check(px, py, pz, n, block_off, ghost_off, sig_off, iters, &ctas_per_pe))) return rc;
   Cfg c = rt().cfg;
   unsigned long long bo = block_off, go = ghost_off, so = sig_off;
   int one = 1, device_barrier = 0;

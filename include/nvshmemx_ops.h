@@ -124,7 +124,8 @@ int nvshmemx_op_alltoall_host(int op, int dtype, size_t send_off, size_t recv_of
  * receiver gets from its -x neighbour goes to its -x ghost), then quiets,
  * sets the neighbour's signal (int at sig_off + 4*face) to it+1 with
  * nvshmem_int_p, waits for its own 6 signals with nvshmem_int_wait_until,
- * and meets the others at the device barrier. */
+ * and meets the others at the device barrier.  ctas_per_pe 0 launches as
+ * many CTAs per PE as stay co-resident. */
 int nvshmemx_op_halo(int px, int py, int pz, int n, size_t block_off, size_t ghost_off,
                      size_t sig_off, int iters, int ctas_per_pe, float *out_ms);
 /* The same exchange in the prototype's own structure: one collective launch
