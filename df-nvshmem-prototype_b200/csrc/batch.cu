@@ -56,19 +56,30 @@ __device__ __forceinline__ void pdl_wait_prerequisites() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
+// Start of an exec kernel: `ctl` holds the piece's plan status, `sctl` the
+// status the host reads (the same block for one piece; the first piece's
+// for the second piece of a pipelined submit, which runs after the first
+// piece is done).  A plan error of this piece is copied to `sctl` (first
+// error wins); the piece runs only if neither reports an error.
+__device__ __forceinline__ bool piece_may_run(BatchCtl *ctl, BatchCtl *sctl) {
+  const int own = *(volatile int *)&ctl->status;
+  if (ctl != sctl && own != 0 && blockIdx.x == 0 && threadIdx.x == 0)
+    set_status(sctl, own, *(volatile int *)&ctl->bad_request);
+  return own == 0 && *(volatile int *)&sctl->status == 0;
+}
+
 // ------------------------------------------------------------------- plan
-// A batch is planned as one piece, or (pipelined submit) as consecutive
-// pieces: piece p appends its items after those of piece p-1 (`prev`, planned
-// earlier on the same stream) and reports errors, with request indices
-// offset by `req_base`, in the first piece's control block `sctl`.
+// A batch is planned as one piece, or (pipelined submit) as two pieces, each
+// writing its items into its own region of the table, [ibase, cap_end), and
+// reporting errors, with request indices offset by `req_base`, in the first
+// piece's control block `sctl`.
 __global__ void __launch_bounds__(256) batch_plan_kernel(Cfg c, const nvshmemx_request *__restrict__ reqs, int n,
                                                          unsigned chunk, WorkItem *__restrict__ items,
                                                          unsigned long long cap, BatchCtl *ctl, BatchCtl *sctl,
-                                                         const BatchCtl *prev, int req_base) {
+                                                         unsigned long long ibase, int req_base) {
   __shared__ unsigned warp_sums[8];
   __shared__ unsigned long long block_base;
   pdl_release_dependents();
-  const unsigned long long ibase = prev ? prev->item_base + prev->total_chunks : 0ull;
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->item_base = ibase;
   const int i = blockIdx.x * 256 + threadIdx.x;
   const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -192,10 +203,10 @@ __device__ __forceinline__ void run_item(const WorkItem &w, unsigned lane) {
 
 template <int VB, int U>
 __global__ void __launch_bounds__(1024) batch_exec_kernel(const WorkItem *__restrict__ items, BatchCtl *ctl,
-                                                          const BatchCtl *sctl, unsigned long long cap, int grab) {
+                                                          BatchCtl *sctl, unsigned long long cap, int grab) {
   const unsigned lane = threadIdx.x & 31u;
   pdl_wait_prerequisites();
-  if (*(volatile const int *)&sctl->status != 0) return;
+  if (!piece_may_run(ctl, sctl)) return;
   unsigned long long C = *(volatile unsigned long long *)&ctl->total_chunks;
   const unsigned long long ib = *(volatile unsigned long long *)&ctl->item_base;
   if (ib + C > cap) return;
@@ -337,7 +348,7 @@ __global__ void __launch_bounds__(256) batch_exec_tma_kernel(const WorkItem *__r
   pdl_wait_prerequisites();
   unsigned long long C = *(volatile unsigned long long *)&ctl->total_chunks;
   const unsigned long long ib = *(volatile unsigned long long *)&ctl->item_base;
-  if (*(volatile int *)&sctl->status != 0 || ib + C > cap) C = 0;  // nothing to run
+  if (!piece_may_run(ctl, sctl) || ib + C > cap) C = 0;  // nothing to run
   items += ib;
   unsigned long long bse = 0;
   if (lane == 0) bse = atomicAdd(&ctl->cursor, (unsigned long long)grab);
@@ -650,7 +661,7 @@ static const void *stream_fn(int stages) {
   }
 }
 
-typedef void (*ExecFn)(const WorkItem *, BatchCtl *, const BatchCtl *, unsigned long long, int);
+typedef void (*ExecFn)(const WorkItem *, BatchCtl *, BatchCtl *, unsigned long long, int);
 
 static ExecFn pick_exec(int vb, int u) {
 #define NVSHM_PICK(V, UU) \
@@ -762,20 +773,28 @@ static int enqueue_stream(nvshmemx_batch *b, bool with_events, const nvshmemx_re
   return check_cuda(cudaGetLastError(), "batch streaming launch");
 }
 
-// Plan + exec of one piece of a batch (n requests at `src`) on stream `st`,
-// with the piece's control block `ctl`, errors into `sctl`, and the items
-// appended after those of `prev` (nullptr: the first piece).
+// Plan (parts & 1) and/or exec (parts & 2) of one piece of a batch (n
+// requests at `src`) on stream `st`, with the piece's control block `ctl`,
+// errors into `sctl`, and its items in [ibase, ibase + cap) of the table.
+enum { kPlan = 1, kExec = 2 };
 static int enqueue_piece(nvshmemx_batch *b, bool with_events, const nvshmemx_request *src, int n, BatchCtl *ctl,
-                         BatchCtl *sctl, const BatchCtl *prev, int req_base, cudaStream_t st) {
+                         BatchCtl *sctl, unsigned long long ibase, int req_base, cudaStream_t st, int parts) {
   const Runtime &r = rt();
   const Cfg c = r.cfg;
   const nvshmemx_batch_config &k = b->cfg;
+  const unsigned long long cap_end = ibase + b->cap;
   ExecFn fn = pick_exec(k.vec_bytes, k.unroll);
   TmaFn tfn = k.tma_stages ? pick_tma(k.tma_stages) : nullptr;
   if (!fn || (k.tma_stages && !tfn))
     return fail(NVSHMEMX_ERR_INVALID, "batch: no kernel for vec %d unroll %d stages %d", k.vec_bytes, k.unroll,
                 k.tma_stages);
   (void)cudaGetLastError();  // report only this enqueue's own launch errors
+  if (with_events) cudaEventRecord(b->ev_plan0, st);
+  if ((parts & kPlan) && n > 0)
+    batch_plan_kernel<<<(n + 255) / 256, 256, 0, st>>>(c, src, n, (unsigned)k.chunk_bytes, b->d_items, cap_end, ctl,
+                                                       sctl, ibase, req_base);
+  if (with_events) cudaEventRecord(b->ev_exec0, st);
+  if (!(parts & kExec)) return check_cuda(cudaGetLastError(), "batch plan launch");
   const size_t smem = tfn ? tma_smem_bytes(k) : 0;
   int per_sm = 0;
   if (tfn) {
@@ -786,11 +805,6 @@ static int enqueue_piece(nvshmemx_batch *b, bool with_events, const nvshmemx_req
   }
   if (per_sm < 1) per_sm = 1;
   int ctas = k.ctas_per_sm > 0 && k.ctas_per_sm < per_sm ? k.ctas_per_sm : per_sm;
-  if (with_events) cudaEventRecord(b->ev_plan0, st);
-  if (n > 0)
-    batch_plan_kernel<<<(n + 255) / 256, 256, 0, st>>>(c, src, n, (unsigned)k.chunk_bytes, b->d_items, b->cap, ctl,
-                                                       sctl, prev, req_base);
-  if (with_events) cudaEventRecord(b->ev_exec0, st);
   // Right after the plan kernel (no event between them), the exec kernel is
   // a programmatic dependent launch: its set-up overlaps the plan's tail.
   cudaLaunchConfig_t lc = {};
@@ -802,13 +816,13 @@ static int enqueue_piece(nvshmemx_batch *b, bool with_events, const nvshmemx_req
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   lc.attrs = attr;
-  lc.numAttrs = (n > 0 && !with_events) ? 1 : 0;
+  lc.numAttrs = ((parts & kPlan) && n > 0 && !with_events) ? 1 : 0;
   cudaError_t e;
   if (tfn)
-    e = cudaLaunchKernelEx(&lc, tfn, (const WorkItem *)b->d_items, ctl, sctl, b->cap, k.grab,
+    e = cudaLaunchKernelEx(&lc, tfn, (const WorkItem *)b->d_items, ctl, sctl, cap_end, k.grab,
                            (unsigned)k.tma_stage_bytes, (unsigned)k.tma_min_bytes, (long long)c.wait_timeout_ns);
   else
-    e = cudaLaunchKernelEx(&lc, fn, (const WorkItem *)b->d_items, ctl, (const BatchCtl *)sctl, b->cap, k.grab);
+    e = cudaLaunchKernelEx(&lc, fn, (const WorkItem *)b->d_items, ctl, sctl, cap_end, k.grab);
   if (with_events) cudaEventRecord(b->ev_exec1, st);
   if (e != cudaSuccess) return check_cuda(e, "batch exec launch");
   return check_cuda(cudaGetLastError(), "batch launch");
@@ -820,7 +834,7 @@ static int enqueue_piece(nvshmemx_batch *b, bool with_events, const nvshmemx_req
 static int enqueue_batch(nvshmemx_batch *b, bool with_events, const nvshmemx_request *src) {
   if (b->cfg.stream) return enqueue_stream(b, with_events, src);
   cudaMemsetAsync(b->d_ctl, 0, sizeof(BatchCtl), b->stream);
-  return enqueue_piece(b, with_events, src, b->n, b->d_ctl, b->d_ctl, nullptr, 0, b->stream);
+  return enqueue_piece(b, with_events, src, b->n, b->d_ctl, b->d_ctl, 0, 0, b->stream, kPlan | kExec);
 }
 
 static int ensure_graph(nvshmemx_batch *b, const nvshmemx_request *src) {
@@ -884,7 +898,7 @@ int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes
   if (b->cfg.chunk_bytes < min_chunk_bytes) b->cfg.chunk_bytes = (min_chunk_bytes + 255) / 256 * 256;
   int rc = 0;
   if ((rc = check_cuda(cudaMalloc(&b->d_reqs, (size_t)max_requests * sizeof(nvshmemx_request)), "cudaMalloc(reqs)")) ||
-      (rc = check_cuda(cudaMalloc(&b->d_items, (size_t)b->cap * sizeof(WorkItem)), "cudaMalloc(items)")) ||
+      (rc = check_cuda(cudaMalloc(&b->d_items, 2 * (size_t)b->cap * sizeof(WorkItem)), "cudaMalloc(items)")) ||
       (rc = check_cuda(cudaMalloc(&b->d_ctl, 128), "cudaMalloc(ctl)")) ||
       (rc = check_cuda(cudaMallocHost(&b->h_reqs, (size_t)max_requests * sizeof(nvshmemx_request)),
                        "cudaMallocHost(reqs)")) ||
@@ -904,7 +918,7 @@ int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes
   // control block (BatchCtl or StreamCtl) and every work item's generation
   // tag start at zero; streaming generations start at 1
   cudaMemset(b->d_ctl, 0, 128);
-  cudaMemset(b->d_items, 0, (size_t)b->cap * sizeof(WorkItem));
+  cudaMemset(b->d_items, 0, 2 * (size_t)b->cap * sizeof(WorkItem));
   *out = b;
   return 0;
 }
@@ -984,9 +998,11 @@ int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n
   b->timed_direct = false;
   cudaEventRecord(b->ev_start, b->stream);
   if (n0) {
-    // Two pieces: the first quarter is copied, planned and executed while
-    // the copy stream brings the rest; the second piece is planned (its
-    // items appended after the first's) and executed once both are done.
+    // Two pieces, each with its own control block and region of the item
+    // table.  The batch's stream copies, plans and executes the first
+    // quarter; meanwhile the copy stream brings the rest and plans it (the
+    // plan kernel fits beside the running exec kernel); the second exec
+    // follows the first once that plan is done.
     BatchCtl *c0 = b->d_ctl, *c1 = second_ctl(b);
     if ((rc = check_cuda(cudaMemsetAsync(c0, 0, sizeof(BatchCtl), b->stream), "cudaMemsetAsync")) ||
         (rc = check_cuda(cudaMemsetAsync(c1, 0, sizeof(BatchCtl), b->stream), "cudaMemsetAsync")) ||
@@ -998,10 +1014,11 @@ int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n
         (rc = check_cuda(cudaMemcpyAsync(b->d_reqs + n0, reqs + n0, (size_t)(n - n0) * sizeof(nvshmemx_request),
                                          cudaMemcpyHostToDevice, b->copy_stream),
                          "cudaMemcpyAsync(requests)")) ||
+        (rc = enqueue_piece(b, false, b->d_reqs + n0, n - n0, c1, c1, b->cap, n0, b->copy_stream, kPlan)) ||
         (rc = check_cuda(cudaEventRecord(b->ev_copied, b->copy_stream), "cudaEventRecord")) ||
-        (rc = enqueue_piece(b, false, b->d_reqs, n0, c0, c0, nullptr, 0, b->stream)) ||
+        (rc = enqueue_piece(b, false, b->d_reqs, n0, c0, c0, 0, 0, b->stream, kPlan | kExec)) ||
         (rc = check_cuda(cudaStreamWaitEvent(b->stream, b->ev_copied, 0), "cudaStreamWaitEvent")) ||
-        (rc = enqueue_piece(b, false, b->d_reqs + n0, n - n0, c1, c0, c0, n0, b->stream))) {
+        (rc = enqueue_piece(b, false, b->d_reqs + n0, n - n0, c1, c0, b->cap, n0, b->stream, kExec))) {
       cudaStreamSynchronize(b->copy_stream);
       cudaStreamSynchronize(b->stream);
       return rc;
@@ -1187,7 +1204,7 @@ extern "C" int nvshmemx_batch_execute_noalloc(const nvshmemx_request *d_reqs, in
   if ((rc = check_cuda(cudaMemsetAsync(ctl, 0, sizeof(BatchCtl), s), "cudaMemsetAsync(noalloc control)"))) return rc;
   if (n > 0)
     batch_plan_kernel<<<(n + 255) / 256, 256, 0, s>>>(r.cfg, d_reqs, n, (unsigned)k.chunk_bytes, items,
-                                                      kNoallocMaxItems, ctl, ctl, nullptr, 0);
+                                                      kNoallocMaxItems, ctl, ctl, 0ull, 0);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, k.threads, 0);
   if (per_sm < 1) per_sm = 1;
