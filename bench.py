@@ -447,9 +447,9 @@ def run_gpu(args, rank, world, local):
         "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(len(reqs) * 32),
                 "d2h_bytes_per_step": 8,
                 "mode": "pipelined: the first quarter of the requests executes while the rest is copied"},
-        # plan + exec per device-resident step, 2 x (plan + exec) per
-        # pipelined end-to-end step
-        "gpu_launches": 2 * args.steps + 4 * args.steps,
+        # plan + exec per device-resident step; 2 x (plan + exec) + the
+        # status kernel per pipelined end-to-end step
+        "gpu_launches": 2 * args.steps + 5 * args.steps,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 3), "traffic": traffic,
                      "kernel": ("batch_exec_tma_kernel" if cfg_used.get("tma_stages") else "batch_exec_kernel"),

@@ -205,6 +205,7 @@ template <int VB, int U>
 __global__ void __launch_bounds__(1024) batch_exec_kernel(const WorkItem *__restrict__ items, BatchCtl *ctl,
                                                           BatchCtl *sctl, unsigned long long cap, int grab) {
   const unsigned lane = threadIdx.x & 31u;
+  pdl_release_dependents();
   pdl_wait_prerequisites();
   if (!piece_may_run(ctl, sctl)) return;
   unsigned long long C = *(volatile unsigned long long *)&ctl->total_chunks;
@@ -345,6 +346,7 @@ __global__ void __launch_bounds__(256) batch_exec_tma_kernel(const WorkItem *__r
   const unsigned lane = threadIdx.x & 31u;
   WarpTma<S> ring;
   ring.init(smem, SB, min_bulk, timeout_ns, lane);  // overlaps the plan kernel
+  pdl_release_dependents();
   pdl_wait_prerequisites();
   unsigned long long C = *(volatile unsigned long long *)&ctl->total_chunks;
   const unsigned long long ib = *(volatile unsigned long long *)&ctl->item_base;
@@ -599,6 +601,19 @@ __global__ void __launch_bounds__(256) batch_stream_kernel(Cfg c, const nvshmemx
   }
 }
 
+// End of a pipelined submit: once the last exec kernel is done (it lets this
+// kernel start early; griddepcontrol.wait holds it until the exec grid has
+// completed and its writes are visible), writes the batch status word and
+// the first bad request into the caller-visible pinned host words.
+__global__ void status_to_host_kernel(const BatchCtl *ctl, volatile int *host_status) {
+  pdl_wait_prerequisites();
+  if (threadIdx.x == 0) {
+    host_status[0] = *(volatile const int *)&ctl->status;
+    host_status[1] = *(volatile const int *)&ctl->bad_request;
+    __threadfence_system();
+  }
+}
+
 // Zeroes the control block of a streaming launch and moves its generation
 // on (one thread; a graph node in place of a memset).
 __global__ void stream_reset_kernel(StreamCtl *ctl) {
@@ -708,6 +723,7 @@ struct nvshmemx_batch {
   BatchCtl *d_ctl = nullptr;
   nvshmemx_request *h_reqs = nullptr;  // pinned
   int *h_status = nullptr;             // pinned
+  int *h_status_dev = nullptr;         // h_status as the device sees it
   int n = 0;
   nvshmemx_batch_config cfg{};
   cudaStream_t stream = nullptr;
@@ -915,6 +931,12 @@ int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes
   cudaEventCreate(&b->ev_exec1);
   cudaEventCreateWithFlags(&b->ev_reset, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&b->ev_copied, cudaEventDisableTiming);
+  void *hs = nullptr;
+  if ((rc = check_cuda(cudaHostGetDevicePointer(&hs, b->h_status, 0), "cudaHostGetDevicePointer(status)"))) {
+    nvshmemx_batch_destroy(b);
+    return rc;
+  }
+  b->h_status_dev = static_cast<int *>(hs);
   // control block (BatchCtl or StreamCtl) and every work item's generation
   // tag start at zero; streaming generations start at 1
   cudaMemset(b->d_ctl, 0, 128);
@@ -1005,12 +1027,12 @@ int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n
     // follows the first once that plan is done.
     BatchCtl *c0 = b->d_ctl, *c1 = second_ctl(b);
     if ((rc = check_cuda(cudaMemsetAsync(c0, 0, sizeof(BatchCtl), b->stream), "cudaMemsetAsync")) ||
-        (rc = check_cuda(cudaMemsetAsync(c1, 0, sizeof(BatchCtl), b->stream), "cudaMemsetAsync")) ||
         (rc = check_cuda(cudaMemcpyAsync(b->d_reqs, reqs, (size_t)n0 * sizeof(nvshmemx_request),
                                          cudaMemcpyHostToDevice, b->stream),
                          "cudaMemcpyAsync(requests)")) ||
         (rc = check_cuda(cudaEventRecord(b->ev_reset, b->stream), "cudaEventRecord")) ||
         (rc = check_cuda(cudaStreamWaitEvent(b->copy_stream, b->ev_reset, 0), "cudaStreamWaitEvent")) ||
+        (rc = check_cuda(cudaMemsetAsync(c1, 0, sizeof(BatchCtl), b->copy_stream), "cudaMemsetAsync")) ||
         (rc = check_cuda(cudaMemcpyAsync(b->d_reqs + n0, reqs + n0, (size_t)(n - n0) * sizeof(nvshmemx_request),
                                          cudaMemcpyHostToDevice, b->copy_stream),
                          "cudaMemcpyAsync(requests)")) ||
@@ -1023,16 +1045,31 @@ int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n
       cudaStreamSynchronize(b->stream);
       return rc;
     }
+    // the status word reaches the host from a kernel that starts while the
+    // last exec runs and writes as soon as it is done (no copy to schedule)
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(1);
+    lc.blockDim = dim3(32);
+    lc.stream = b->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    if ((rc = check_cuda(cudaLaunchKernelEx(&lc, status_to_host_kernel, (const BatchCtl *)c0,
+                                            (volatile int *)b->h_status_dev),
+                         "status kernel launch")))
+      return rc;
   } else {
     if (n && (rc = check_cuda(cudaMemcpyAsync(b->d_reqs, reqs, (size_t)n * sizeof(nvshmemx_request),
                                               cudaMemcpyHostToDevice, b->stream),
                               "cudaMemcpyAsync(requests)")))
       return rc;
     if ((rc = check_cuda(cudaGraphLaunch(b->gexec, b->stream), "cudaGraphLaunch"))) return rc;
+    if ((rc = check_cuda(cudaMemcpyAsync(b->h_status, &b->d_ctl->status, 8, cudaMemcpyDeviceToHost, b->stream),
+                         "cudaMemcpyAsync(status)")))
+      return rc;
   }
-  if ((rc = check_cuda(cudaMemcpyAsync(b->h_status, &b->d_ctl->status, 8, cudaMemcpyDeviceToHost, b->stream),
-                       "cudaMemcpyAsync(status)")))
-    return rc;
   cudaEventRecord(b->ev_stop, b->stream);
   if ((rc = check_cuda(cudaStreamSynchronize(b->stream), "batch_submit"))) return rc;
   float ms = 0;

@@ -91,7 +91,8 @@ int nvshmemx_batch_execute(nvshmemx_batch *b, int reps, float *out_ms);
  * the copy precedes the plan and exec kernels on the batch's stream; from
  * 8192 requests on, the batch runs as two pieces: the first quarter (in
  * whole 256-request blocks) is copied, planned and executed while a second
- * stream copies and plans the rest, which executes after the first.  An
+ * stream copies and plans the rest, which executes after the first, and a
+ * one-thread kernel writes the status word into pinned host memory.  An
  * invalid request in the second piece is reported after the first piece has
  * run (with one piece, nothing runs).  In stream mode the copy precedes the
  * streaming kernel.  The requests stay resident: nvshmemx_batch_execute
