@@ -108,3 +108,20 @@ def test_every_device_function_links_against_static_lib(tmp_path):
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-3000:]
     assert out.exists()
+
+
+@pytest.mark.skipif(subprocess.run(["which", "nvcc"], capture_output=True).returncode != 0, reason="no nvcc")
+def test_every_device_function_links_with_device_lto(tmp_path):
+    """The static library also carries LTO IR: an application compiled with
+    code=lto_100a and linked with -dlto gets the device calls inlined."""
+    src = os.path.join(NATIVE, "api_all.cu")
+    obj, out = tmp_path / "api_all.o", tmp_path / "api_all_lto"
+    lib = os.path.join(PKG, "lib")
+    r = subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=lto_100a", "-rdc=true", "-I", INC, "-c", src,
+                        "-o", str(obj)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-3000:]
+    r = subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-dlto", "-rdc=true", str(obj),
+                        "-o", str(out), "-L", lib, "-lnvshmem", "-L/usr/local/cuda/lib64/stubs", "-lcuda"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-3000:]
+    assert out.exists()

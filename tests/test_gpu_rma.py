@@ -102,7 +102,8 @@ def test_signal_values(shmem_factory):
     assert first_diff(heap_images(sh, 3, HEAP), om.heap) is None
 
 
-def test_direct_loads_and_stores_through_nvshmem_ptr(tmp_path):
+@pytest.mark.parametrize("link", ["plain", "dlto"])
+def test_direct_loads_and_stores_through_nvshmem_ptr(tmp_path, link):
     """A CUDA application compiled against libnvshmem.a dereferences the
     addresses nvshmem_ptr (host) and nvshmemx_ptr (device) return: plain
     stores into the next PE's slice, quiet + device barrier, plain loads from
@@ -113,11 +114,20 @@ def test_direct_loads_and_stores_through_nvshmem_ptr(tmp_path):
     import subprocess
     repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     exe = tmp_path / "ptr_direct"
-    r = subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-rdc=true",
-                        "-I", os.path.join(repo, "include"), os.path.join(repo, "tests", "native", "ptr_direct.cu"),
-                        "-o", str(exe), "-L", os.path.join(repo, "df-nvshmem-prototype_b200", "lib"), "-lnvshmem",
-                        "-L/usr/local/cuda/lib64/stubs", "-lcuda"], capture_output=True, text=True, timeout=600)
-    assert r.returncode == 0, r.stderr[-3000:]
+    src = os.path.join(repo, "tests", "native", "ptr_direct.cu")
+    libs = ["-L", os.path.join(repo, "df-nvshmem-prototype_b200", "lib"), "-lnvshmem",
+            "-L/usr/local/cuda/lib64/stubs", "-lcuda"]
+    inc = ["-I", os.path.join(repo, "include")]
+    if link == "plain":
+        cmds = [["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-rdc=true", *inc, src, "-o", str(exe), *libs]]
+    else:  # the application's kernels and the library's device code optimised together
+        obj = str(tmp_path / "ptr_direct.o")
+        cmds = [["nvcc", "-gencode", "arch=compute_100a,code=lto_100a", "-rdc=true", *inc, "-c", src, "-o", obj],
+                ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-dlto", "-rdc=true", obj, "-o", str(exe),
+                 *libs]]
+    for cmd in cmds:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-3000:]
     npes, heap = 4, 1 << 20
     env = dict(os.environ, NVSHMEM_NPES=str(npes), NVSHMEM_HEAP_SIZE=str(heap))
     out = tmp_path / "heaps.bin"
