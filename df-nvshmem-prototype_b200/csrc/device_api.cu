@@ -80,14 +80,14 @@ __device__ void nvshmem_trace_begin(void) {
   const Cfg &c = CFG;
   if (c.trace) {
     unsigned long long t = nvshm::gtimer();
-    nvshm::trace_rec(c, NVSHMEMX_TRACE_BEGIN, nullptr, nullptr, 0, nvshm::my_pe(), t, t);
+    nvshm::trace_rec(c, NVSHMEMX_TRACE_BEGIN, nullptr, nullptr, 0, nvshm::my_pe(CFG), t, t);
   }
 }
 __device__ void nvshmem_trace_end(void) {
   const Cfg &c = CFG;
   if (c.trace) {
     unsigned long long t = nvshm::gtimer();
-    nvshm::trace_rec(c, NVSHMEMX_TRACE_END, nullptr, nullptr, 0, nvshm::my_pe(), t, t);
+    nvshm::trace_rec(c, NVSHMEMX_TRACE_END, nullptr, nullptr, 0, nvshm::my_pe(CFG), t, t);
   }
 }
 
@@ -179,7 +179,7 @@ __device__ void nvshmem_int_wait(int *ivar, int cmp_value) {
   const Cfg &c = CFG;
   unsigned long long t0 = c.trace ? nvshm::gtimer() : 0;
   nvshm::wait_cmp(c, ivar, NVSHMEMX_CMP_NE, cmp_value, 0);
-  if (c.trace) nvshm::trace_rec(c, NVSHMEMX_TRACE_WAIT_INT, ivar, nullptr, 4, nvshm::my_pe(), t0, nvshm::gtimer());
+  if (c.trace) nvshm::trace_rec(c, NVSHMEMX_TRACE_WAIT_INT, ivar, nullptr, 4, nvshm::my_pe(CFG), t0, nvshm::gtimer());
 }
 
 // nvshmem_device.cu:564-584: returns once *ivar == cmp_value; `cmp` is
@@ -190,11 +190,11 @@ __device__ void nvshmem_int_wait_until(int *ivar, int cmp, int cmp_value) {
   unsigned long long t0 = c.trace ? nvshm::gtimer() : 0;
   nvshm::wait_cmp(c, ivar, NVSHMEMX_CMP_EQ, cmp_value, 0);
   if (c.trace)
-    nvshm::trace_rec(c, NVSHMEMX_TRACE_WAIT_UNTIL_INT, ivar, nullptr, 4, nvshm::my_pe(), t0, nvshm::gtimer());
+    nvshm::trace_rec(c, NVSHMEMX_TRACE_WAIT_UNTIL_INT, ivar, nullptr, 4, nvshm::my_pe(CFG), t0, nvshm::gtimer());
 }
 
 // ---------------------------------------------------------------- extensions
-__device__ int nvshmemx_my_pe(void) { return nvshm::my_pe(); }
+__device__ int nvshmemx_my_pe(void) { return nvshm::my_pe(CFG); }
 __device__ int nvshmemx_n_pes(void) { return CFG.npes; }
 
 __device__ void *nvshmemx_ptr(const void *sym, int pe) {
@@ -202,7 +202,7 @@ __device__ void *nvshmemx_ptr(const void *sym, int pe) {
   if (!nvshm::in_arena(c, sym) || (unsigned)pe >= (unsigned)c.npes) return nullptr;
   return nvshm::xlate(c, sym, pe);
 }
-__device__ void *nvshmemx_local_ptr(const void *sym) { return nvshmemx_ptr(sym, nvshm::my_pe()); }
+__device__ void *nvshmemx_local_ptr(const void *sym) { return nvshmemx_ptr(sym, nvshm::my_pe(CFG)); }
 
 __device__ void nvshmemx_putmem_warp(void *target, const void *source, size_t bytes, int pe) {
   putmem_coop(target, source, bytes, pe, lane_id(), 32, NVSHMEMX_TRACE_PUT_INT);
@@ -268,7 +268,7 @@ __device__ int nvshmemx_barrier_all(void) {
   unsigned long long t0 = c.trace ? nvshm::gtimer() : 0;
   int rc = nvshm::barrier_all(c);
   if (c.trace && nvshm::block_rank() == 0)
-    nvshm::trace_rec(c, NVSHMEMX_TRACE_BARRIER, nullptr, nullptr, 0, nvshm::my_pe(), t0, nvshm::gtimer());
+    nvshm::trace_rec(c, NVSHMEMX_TRACE_BARRIER, nullptr, nullptr, 0, nvshm::my_pe(CFG), t0, nvshm::gtimer());
   return rc;
 }
 __device__ int nvshmemx_barrier_pe(void) { return nvshm::barrier_pe(CFG); }
@@ -279,7 +279,7 @@ __device__ int nvshmemx_barrier_all_ep(unsigned long long episode) {
   const unsigned long long P = (unsigned long long)gridDim.x * gridDim.y * gridDim.z;
   int rc = nvshm::episode_barrier(c, c.coll_bar, P, episode);
   if (c.trace && nvshm::block_rank() == 0)
-    nvshm::trace_rec(c, NVSHMEMX_TRACE_BARRIER, nullptr, nullptr, 0, nvshm::my_pe(), t0, nvshm::gtimer());
+    nvshm::trace_rec(c, NVSHMEMX_TRACE_BARRIER, nullptr, nullptr, 0, nvshm::my_pe(CFG), t0, nvshm::gtimer());
   return rc;
 }
 

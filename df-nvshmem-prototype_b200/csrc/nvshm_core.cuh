@@ -38,7 +38,8 @@ struct Cfg {
   nvshmemx_trace_record *trace;    // npes * trace_cap records, or nullptr
   unsigned long long *trace_head;  // per-PE record counters
   unsigned int trace_cap;          // power of two
-  int pad_;
+  int proc_pe;                     // process-per-PE mode: this process's PE; -1
+                                   // when all PEs share one collective launch
 };
 
 // ---------------------------------------------------------------- PTX helpers
@@ -91,7 +92,9 @@ __device__ __forceinline__ unsigned smem_u32(const void *p) {
 }
 
 // ------------------------------------------------------------- PE / addresses
-__device__ __forceinline__ int my_pe() { return (int)blockIdx.z; }
+// The calling PE: blockIdx.z of a collective launch, or the process's PE when
+// every PE is a process of its own.
+__device__ __forceinline__ int my_pe(const Cfg &c) { return c.proc_pe >= 0 ? c.proc_pe : (int)blockIdx.z; }
 
 __device__ __forceinline__ bool in_arena(const Cfg &c, const void *p) {
   return (unsigned long long)((const char *)p - c.arena) < c.arena_bytes;
@@ -108,7 +111,7 @@ __device__ __forceinline__ char *xlate(const Cfg &c, const void *sym, int pe) {
 // Records the first device-side error; later ones are dropped.
 __device__ __forceinline__ void record_error(const Cfg &c, int code, long long detail) {
   if (atomicCAS(c.status, 0, code) == 0) {
-    c.status[1] = my_pe();
+    c.status[1] = my_pe(c);
     *(volatile long long *)(c.status + 2) = detail;
   }
 }
@@ -137,7 +140,7 @@ __device__ __forceinline__ bool check_local(const Cfg &c, const void *p, unsigne
 __device__ __forceinline__ void trace_rec(const Cfg &c, int op, const void *local,
                                           const void *remote, unsigned long long bytes, int peer,
                                           unsigned long long t0, unsigned long long t1) {
-  int pe = my_pe();
+  int pe = my_pe(c);
   if ((unsigned)pe >= (unsigned)c.npes) pe = 0;
   unsigned long long idx = atomicAdd(&c.trace_head[pe], 1ull);
   nvshmemx_trace_record *r =
@@ -480,7 +483,7 @@ __device__ __forceinline__ int barrier_all(const Cfg &c) {
 }
 
 __device__ __forceinline__ int barrier_pe(const Cfg &c) {
-  int pe = my_pe();
+  int pe = my_pe(c);
   if ((unsigned)pe >= (unsigned)c.npes) pe = 0;
   const unsigned long long P = (unsigned long long)gridDim.x * gridDim.y;
   return ticket_barrier(c, c.pe_bar + (size_t)pe * 16, P);  // counters 128 bytes apart

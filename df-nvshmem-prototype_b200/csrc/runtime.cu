@@ -19,6 +19,8 @@
 #include <string.h>
 #include <unistd.h>
 
+#include "procs.h"
+
 #include <chrono>
 #include <condition_variable>
 #include <string>
@@ -87,6 +89,9 @@ struct DriverApi {
   PFN_cuMemMap map = nullptr;
   PFN_cuMemUnmap unmap = nullptr;
   PFN_cuMemSetAccess set_access = nullptr;
+  // process-per-PE mode only
+  PFN_cuMemExportToShareableHandle export_handle = nullptr;
+  PFN_cuMemImportFromShareableHandle import_handle = nullptr;
   bool loaded = false;
 };
 static DriverApi g_drv;
@@ -109,6 +114,8 @@ static int load_driver() {
             get_entry("cuMemUnmap", (void **)&g_drv.unmap) &&
             get_entry("cuMemSetAccess", (void **)&g_drv.set_access);
   if (!ok) return fail(NVSHMEMX_ERR_CUDA, "cannot resolve the CUDA driver's virtual-memory entry points");
+  get_entry("cuMemExportToShareableHandle", (void **)&g_drv.export_handle);
+  get_entry("cuMemImportFromShareableHandle", (void **)&g_drv.import_handle);
   g_drv.loaded = true;
   return 0;
 }
@@ -205,6 +212,7 @@ static void release_all() {
   r.ctrl = nullptr;
   if (r.arena) {
     for (int p = 0; p < (int)r.handles.size(); ++p) {
+      if (!r.handles[p]) continue;
       g_drv.unmap((CUdeviceptr)(r.arena + (size_t)p * r.stride), r.slice_mapped);
       g_drv.release(r.handles[p]);
     }
@@ -215,7 +223,51 @@ static void release_all() {
   r.started = false;
 }
 
-static int init_impl(int npes, size_t heap) {
+// Process-per-PE mode: create this process's slice as an exportable
+// allocation, exchange descriptors with the other PE processes, and map every
+// slice at its place in the arena.  The own slice is zeroed, then all PEs
+// meet, so no PE writes into a slice before its owner has cleared it.
+static int map_process_slices(int pe, int npes, const char *dir, const CUmemAllocationProp &prop,
+                              const CUmemAccessDesc &acc) {
+  Runtime &r = rt();
+  int rc;
+  if ((rc = proc_open(pe, npes, dir))) return rc;
+  const double timeout = host_barrier_timeout_s();
+  CUdeviceptr base = (CUdeviceptr)r.arena;
+  if ((rc = check_cu(g_drv.create(&r.handles[pe], r.slice_mapped, &prop, 0), "cuMemCreate"))) return rc;
+  int my_fd = -1;
+  if ((rc = check_cu(g_drv.export_handle(&my_fd, r.handles[pe], CU_MEM_HANDLE_TYPE_POSIX_FILE_DESCRIPTOR, 0),
+                     "cuMemExportToShareableHandle")))
+    return rc;
+  std::vector<int> fds;
+  rc = proc_exchange_fds(my_fd, fds, timeout);
+  for (int q = 0; q < npes && !rc; ++q) {
+    if (q != pe &&
+        (rc = check_cu(g_drv.import_handle(&r.handles[q], (void *)(uintptr_t)fds[q],
+                                           CU_MEM_HANDLE_TYPE_POSIX_FILE_DESCRIPTOR),
+                       "cuMemImportFromShareableHandle")))
+      break;
+    CUdeviceptr at = base + (size_t)q * r.stride;
+    if ((rc = check_cu(g_drv.map(at, r.slice_mapped, 0, r.handles[q], 0), "cuMemMap")) ||
+        (rc = check_cu(g_drv.set_access(at, r.slice_mapped, &acc, 1), "cuMemSetAccess"))) {
+      g_drv.release(r.handles[q]);
+      r.handles[q] = 0;
+      break;
+    }
+  }
+  for (int fd : fds)
+    if (fd >= 0) close(fd);
+  if (rc) return rc;
+  if ((rc = check_cuda(cudaMemset(r.arena + (size_t)pe * r.stride, 0, r.slice_mapped), "cudaMemset(slice)")) ||
+      (rc = check_cuda(cudaDeviceSynchronize(), "cudaDeviceSynchronize")))
+    return rc;
+  return proc_barrier(timeout);
+}
+
+// proc_pe < 0: every PE in this process (one arena, one collective launch);
+// proc_pe >= 0: this process is PE proc_pe of npes processes meeting in the
+// rendezvous directory `dir` (procs.cu).
+static int init_impl(int npes, size_t heap, int proc_pe = -1, const char *dir = nullptr) {
   Runtime &r = rt();
   std::lock_guard<std::recursive_mutex> lk(r.mu);
   read_env_error_mode();
@@ -234,11 +286,15 @@ static int init_impl(int npes, size_t heap) {
                        "cudaDeviceGetAttribute")))
     return rc;
 
+  const bool procs = proc_pe >= 0;
+  if (procs && (!g_drv.export_handle || !g_drv.import_handle))
+    return fail(NVSHMEMX_ERR_UNSUPPORTED, "process mode: the driver cannot share VMM allocations");
   CUmemAllocationProp prop;
   memset(&prop, 0, sizeof prop);
   prop.type = CU_MEM_ALLOCATION_TYPE_PINNED;
   prop.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
   prop.location.id = r.device;
+  if (procs) prop.requestedHandleTypes = CU_MEM_HANDLE_TYPE_POSIX_FILE_DESCRIPTOR;
   size_t gran = 0;
   if ((rc = check_cu(g_drv.granularity(&gran, &prop, CU_MEM_ALLOC_GRANULARITY_RECOMMENDED),
                      "cuMemGetAllocationGranularity")))
@@ -252,7 +308,7 @@ static int init_impl(int npes, size_t heap) {
 
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
-  if ((size_t)npes * r.slice_mapped > free_b)
+  if ((size_t)(procs ? 1 : npes) * r.slice_mapped > free_b)
     return fail(NVSHMEMX_ERR_NOMEM, "nvstart_pes: %d PEs x %zu bytes exceed free device memory (%zu)", npes,
                 r.slice_mapped, free_b);
 
@@ -267,24 +323,30 @@ static int init_impl(int npes, size_t heap) {
   acc.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
   acc.location.id = r.device;
   acc.flags = CU_MEM_ACCESS_FLAGS_PROT_READWRITE;
-  for (int p = 0; p < npes; ++p) {
-    CUdeviceptr at = base + (size_t)p * r.stride;
-    if ((rc = check_cu(g_drv.create(&r.handles[p], r.slice_mapped, &prop, 0), "cuMemCreate")) ||
-        (rc = check_cu(g_drv.map(at, r.slice_mapped, 0, r.handles[p], 0), "cuMemMap")) ||
-        (rc = check_cu(g_drv.set_access(at, r.slice_mapped, &acc, 1), "cuMemSetAccess"))) {
-      r.handles.resize(p + 1);
-      if (r.handles[p] == 0) r.handles.resize(p);
-      release_all();
-      return rc;
+  if (!procs) {
+    for (int p = 0; p < npes; ++p) {
+      CUdeviceptr at = base + (size_t)p * r.stride;
+      if ((rc = check_cu(g_drv.create(&r.handles[p], r.slice_mapped, &prop, 0), "cuMemCreate")) ||
+          (rc = check_cu(g_drv.map(at, r.slice_mapped, 0, r.handles[p], 0), "cuMemMap")) ||
+          (rc = check_cu(g_drv.set_access(at, r.slice_mapped, &acc, 1), "cuMemSetAccess"))) {
+        r.handles.resize(p + 1);
+        if (r.handles[p] == 0) r.handles.resize(p);
+        release_all();
+        return rc;
+      }
     }
-  }
-  // The prototype leaves its heap uninitialised (cuMemAlloc, nvshmem.cu:504);
-  // zeroing it makes every run start from the same heap image.
-  for (int p = 0; p < npes; ++p) {
-    if ((rc = check_cuda(cudaMemset(r.arena + (size_t)p * r.stride, 0, r.slice_mapped), "cudaMemset(arena)"))) {
-      release_all();
-      return rc;
+    // The prototype leaves its heap uninitialised (cuMemAlloc, nvshmem.cu:504);
+    // zeroing it makes every run start from the same heap image.
+    for (int p = 0; p < npes; ++p) {
+      if ((rc = check_cuda(cudaMemset(r.arena + (size_t)p * r.stride, 0, r.slice_mapped), "cudaMemset(arena)"))) {
+        release_all();
+        return rc;
+      }
     }
+  } else if ((rc = map_process_slices(proc_pe, npes, dir, prop, acc))) {
+    release_all();
+    proc_close();
+    return rc;
   }
 
   // control block: status (64 B), collective counter and per-PE counters each
@@ -316,6 +378,8 @@ static int init_impl(int npes, size_t heap) {
   // per-PE counters are 128 bytes apart: index p*16 in units of u64
   c.pe_bar = r.d_pe_bar;
   c.wait_timeout_ns = r.wait_timeout_ns;
+  c.proc_pe = proc_pe;
+  if (procs) t_pe = proc_pe;
   r.started = true;
   if ((rc = publish_cfg())) {
     release_all();
@@ -362,13 +426,15 @@ int launch_collective(const void *func, dim3 grid, dim3 block, void **args, size
   if ((rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, threads, smem),
                        "cudaOccupancyMaxActiveBlocksPerMultiprocessor")))
     return rc;
-  long long total = (long long)grid.x * grid.y * r.npes;
+  // process mode: the launch carries this process's PE only
+  const int pes = proc_mode() ? 1 : r.npes;
+  long long total = (long long)grid.x * grid.y * pes;
   if (total > (long long)per_sm * r.sm_count)
     return fail(NVSHMEMX_ERR_COOP, "collective launch: %lld CTAs cannot be co-resident (%d per SM x %d SMs)",
                 total, per_sm, r.sm_count);
   if ((rc = check_cuda(cudaMemsetAsync(r.d_coll_bar, 0, r.bar_reset_bytes, stream), "cudaMemsetAsync(barrier)")))
     return rc;
-  dim3 g(grid.x, grid.y, (unsigned)r.npes);
+  dim3 g(grid.x, grid.y, (unsigned)pes);
   return check_cuda(cudaLaunchCooperativeKernel(func, g, block, args, smem, stream), "cudaLaunchCooperativeKernel");
 }
 
@@ -401,7 +467,18 @@ void nvstart_pes(void) {
   // the allocation; here it sizes the allocation too.
   v = getenv("NVSHMEM_HEAP_SIZE");
   if (v) heap = (size_t)atoll(v);
-  init_impl(npes, heap);
+  // One process per PE (the launcher sets these), as under the prototype's
+  // mpirun; otherwise every PE in this process.
+  const char *pp = getenv("NVSHMEM_PROCESS_PE");
+  if (pp)
+    init_impl(npes, heap, atoi(pp), getenv("NVSHMEM_RENDEZVOUS"));
+  else
+    init_impl(npes, heap);
+}
+
+int nvshmemx_init_process(int pe, int npes, size_t heap_bytes_per_pe, const char *rendezvous_dir) {
+  if (pe < 0) return fail(NVSHMEMX_ERR_INVALID, "nvshmemx_init_process: PE %d", pe);
+  return init_impl(npes, heap_bytes_per_pe, pe, rendezvous_dir);
 }
 
 int nvshmemx_finalize(void) {
@@ -409,6 +486,8 @@ int nvshmemx_finalize(void) {
   std::lock_guard<std::recursive_mutex> lk(r.mu);
   if (!r.started) return fail(NVSHMEMX_ERR_STATE, "nvstop_pes: not started");
   int rc = check_cuda(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+  // process mode: nobody unmaps a slice another PE may still write
+  if (proc_mode() && rc == 0) rc = proc_barrier(host_barrier_timeout_s());
   if (r.trace_from_env && r.d_trace && rc == 0) {
     // nvshmem_processed_tracefile_<pid>_<pe>, as the prototype's stop wrote
     // (nvshmem.cu:377)
@@ -416,6 +495,7 @@ int nvshmemx_finalize(void) {
   }
   r.trace_from_env = false;
   release_all();
+  if (proc_mode()) proc_close();
   return rc;
 }
 
@@ -430,7 +510,7 @@ void nvstop_pes(void) {
 
 int nvshmemx_is_started(void) { return rt().started ? 1 : 0; }
 
-int nvshmem_my_pe(void) { return t_pe; }
+int nvshmem_my_pe(void) { return proc_mode() ? proc_pe() : t_pe; }
 int nvshmem_n_pes(void) { return rt().npes; }
 
 // ---------------------------------------------------------------- allocation
@@ -468,7 +548,7 @@ void *nvshmalloc(size_t size) {
     return nullptr;
   }
   for (int p = 0; p < r.npes; ++p) r.tail[p] = off + size;
-  return r.arena + (size_t)t_pe * r.stride + off;
+  return r.arena + (size_t)nvshmem_my_pe() * r.stride + off;
 }
 
 void nvshmcleanup(void) {
@@ -497,6 +577,10 @@ void nvshmem_barrier_all(void) {
     return;
   }
   if (check_cuda(cudaDeviceSynchronize(), "cudaDeviceSynchronize")) return;
+  if (proc_mode()) {
+    proc_barrier(host_barrier_timeout_s());
+    return;
+  }
   if (t_spmd) {
     int rc = g_hbar.wait(host_barrier_timeout_s());
     if (rc) fail(rc, "nvshmem_barrier_all: a PE thread left or the host barrier timed out");
@@ -507,6 +591,12 @@ void nvshmem_barrier_all_offload(void) {
   Runtime &r = rt();
   if (!r.started) {
     fail(NVSHMEMX_ERR_STATE, "nvshmem_barrier_all_offload before nvstart_pes");
+    return;
+  }
+  if (proc_mode()) {
+    // kernels of different processes cannot wait for each other on one GPU:
+    // the PE processes meet on the host
+    nvshmem_barrier_all();
     return;
   }
   if (t_spmd) {
@@ -658,6 +748,7 @@ long long nvshmemx_get_wait_timeout_ns(void) { return rt().wait_timeout_ns; }
 int nvshmemx_spmd_run(void (*fn)(void *), void *arg) {
   Runtime &r = rt();
   if (!r.started) return fail(NVSHMEMX_ERR_STATE, "nvshmemx_spmd_run before nvstart_pes");
+  if (proc_mode()) return fail(NVSHMEMX_ERR_STATE, "nvshmemx_spmd_run: every PE is a process already");
   if (r.spmd_active) return fail(NVSHMEMX_ERR_STATE, "nvshmemx_spmd_run: already running");
   r.spmd_active = true;
   g_hbar.n = r.npes;

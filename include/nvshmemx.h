@@ -81,6 +81,18 @@ extern "C" {
 /* nvstart_pes with explicit values instead of NVSHMEM_NPES/NVSHMEM_HEAP_SIZE;
  * returns a status code instead of exiting. */
 int nvshmemx_init_attr(int npes, size_t heap_bytes_per_pe);
+/* Process-per-PE mode, the prototype's own model (one process per PE, as its
+ * MPI ranks were; nvshmem.cu:472-561): this process becomes PE `pe` of `npes`
+ * processes that meet in the directory `rendezvous_dir`, where they exchange
+ * their slices' VMM handles over Unix sockets and share the host barrier.
+ * Every slice is mapped in every process at the same arena layout, so device
+ * calls work unchanged; nvshmem_barrier_all synchronises the device and meets
+ * the other processes on the host, and nvshmem_barrier_all_offload does the
+ * same (kernels of different processes cannot wait for each other on one GPU,
+ * so device-side waits on another process's data are not supported).
+ * nvstart_pes enters this mode when NVSHMEM_PROCESS_PE and
+ * NVSHMEM_RENDEZVOUS are set (python -m nvshmem_b200.launch sets them). */
+int nvshmemx_init_process(int pe, int npes, size_t heap_bytes_per_pe, const char *rendezvous_dir);
 /* nvstop_pes with a status code. */
 int nvshmemx_finalize(void);
 int nvshmemx_is_started(void);

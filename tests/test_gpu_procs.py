@@ -1,0 +1,66 @@
+"""Process-per-PE mode, the prototype's own execution model: a prototype-style
+application (tests/native/proc_pes.cu, linked against libnvshmem.a) runs as
+one process per PE under python -m nvshmem_b200.launch.  Every process maps
+every PE's slice through exchanged VMM handles; puts and gets between the
+processes must leave the heaps equal to the oracle's, and a PE process that
+leaves must make the others' nvshmem_barrier_all fail instead of waiting."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from nvshmem_b200 import DT_INT, REQ_GET, REQ_PUT
+from nvshmem_b200.launch import launch
+from oracle.model import Model
+from _util import first_diff, requests
+
+pytestmark = pytest.mark.gpu
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def build(tmp_path):
+    exe = tmp_path / "proc_pes"
+    r = subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-rdc=true",
+                        "-I", os.path.join(REPO, "include"), os.path.join(REPO, "tests", "native", "proc_pes.cu"),
+                        "-o", str(exe), "-L", os.path.join(REPO, "df-nvshmem-prototype_b200", "lib"), "-lnvshmem",
+                        "-L/usr/local/cuda/lib64/stubs", "-lcuda"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+    return str(exe)
+
+
+def pattern(pe, n):
+    i = np.arange(n, dtype=np.uint64)
+    return ((pe * 2654435761 + i * 40503 + 7) & 0xFFFFFFFF).astype(np.uint32)
+
+
+@pytest.mark.parametrize("npes", [2, 4])
+def test_processes_exchange_blocks(tmp_path, npes):
+    exe = build(tmp_path)
+    heap = 4 << 20
+    codes = launch([exe, "exchange", str(tmp_path)], npes, heap=heap, timeout=240,
+                   env=dict(os.environ, NVSHMEM_HOST_BARRIER_TIMEOUT_S="60"))
+    assert codes == [0] * npes, codes
+    rows = [list(map(int, (tmp_path / f"pe{pe}.txt").read_text().split())) for pe in range(npes)]
+    assert sorted(r[0] for r in rows) == list(range(npes))
+    _, send, recv, got, n = rows[0]
+    assert all(r[1:] == [send, recv, got, n] for r in rows)  # symmetric offsets in every process
+    images = np.stack([np.fromfile(tmp_path / f"pe{pe}.bin", dtype=np.uint8) for pe in range(npes)])
+    om = Model(npes, heap)
+    for pe in range(npes):
+        om.heap[pe][send:send + 4 * n] = pattern(pe, n).view(np.uint8)
+    ring = [dict(src_off=send, dst_off=recv + p * 4 * n, bytes=4 * n, src_pe=p, dst_pe=(p + 1) % npes, op=REQ_PUT,
+                 dtype=DT_INT) for p in range(npes)]
+    pull = [dict(src_off=send, dst_off=got, bytes=4 * n, src_pe=(p - 1) % npes, dst_pe=p, op=REQ_GET, dtype=DT_INT)
+            for p in range(npes)]
+    om.apply_requests(requests(ring))
+    om.apply_requests(requests(pull))
+    assert first_diff(images, om.heap) is None
+
+
+def test_departed_process_fails_the_barrier(tmp_path):
+    exe = build(tmp_path)
+    codes = launch([exe, "depart", str(tmp_path)], 3, heap=4 << 20, timeout=240, stop_on_failure=False,
+                   env=dict(os.environ, NVSHMEM_HOST_BARRIER_TIMEOUT_S="3"))
+    assert codes == [3, 0, 3], codes
