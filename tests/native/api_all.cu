@@ -77,5 +77,6 @@ int main() {
   printf("%p %d %d\n", nvshmem_ptr(ia, 1), nvshmem_n_pes(), nvshmemx_status());
   nvshmcleanup();
   nvstop_pes();
+  nvshmemx_init_process(0, 2, 1 << 20, "/nonexistent");  // process-per-PE start (returns an error here)
   return 0;
 }
