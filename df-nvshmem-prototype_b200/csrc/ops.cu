@@ -12,6 +12,7 @@
 #include "nvshmem_device.h"
 #include "nvshmemx.h"
 #include "nvshmemx_ops.h"
+#include "procs.h"
 #include "runtime.h"
 
 namespace nvshm {
@@ -430,6 +431,17 @@ static int need_started() {
   return 0;
 }
 
+// The C1-C3 operations run every PE in one collective launch and meet at
+// device barriers; with one process per PE those barriers would see only
+// this process's CTAs, so the operations refuse instead.
+static int need_collective() {
+  int rc;
+  if ((rc = need_started())) return rc;
+  if (proc_mode())
+    return fail(NVSHMEMX_ERR_STATE, "operation needs every PE in one process (one process per PE is active)");
+  return 0;
+}
+
 static int last_launch(const char *what) {
   return check_cuda(cudaGetLastError(), what);
 }
@@ -540,7 +552,7 @@ int nvshmemx_checksum(int pe, size_t off, size_t bytes, unsigned long long *out)
 int nvshmemx_op_pingpong(size_t flag_off, size_t data_off, int len_elems, int iters, int skip, double *out_ns,
                          double *out_total_ns) {
   int rc;
-  if ((rc = need_started())) return rc;
+  if ((rc = need_collective())) return rc;
   const Runtime &r = rt();
   if (r.npes < 2) return fail(NVSHMEMX_ERR_INVALID, "pingpong needs at least 2 PEs");
   if (iters < 1 || skip < 0 || len_elems < 0 || flag_off + 4 > r.heap_bytes ||
@@ -569,7 +581,7 @@ int nvshmemx_op_pingpong(size_t flag_off, size_t data_off, int len_elems, int it
 
 int nvshmemx_op_barrier_latency(int ctas_per_pe, int iters, int counted, double *out_ns, double *out_total_ns) {
   int rc;
-  if ((rc = need_started())) return rc;
+  if ((rc = need_collective())) return rc;
   if (ctas_per_pe < 1 || iters < 1) return fail(NVSHMEMX_ERR_INVALID, "barrier_latency: bad arguments");
   long long *cyc = (long long *)g_out_buf.get((size_t)iters * 8 + 64);
   if (!cyc) return fail(NVSHMEMX_ERR_NOMEM, "barrier scratch");
@@ -593,7 +605,7 @@ int nvshmemx_op_barrier_latency(int ctas_per_pe, int iters, int counted, double 
 
 int nvshmemx_op_offload_barrier(int iters, double *out_us_per_call) {
   int rc;
-  if ((rc = need_started())) return rc;
+  if ((rc = need_collective())) return rc;
   if (iters < 1) return fail(NVSHMEMX_ERR_INVALID, "offload_barrier: iters < 1");
   nvshmem_barrier_all_offload();  // warm-up
   if ((rc = check_cuda(cudaDeviceSynchronize(), "offload barrier"))) return rc;
@@ -612,7 +624,7 @@ static int alltoall_setup(int op, int dtype, size_t send_off, size_t recv_off, s
                           size_t set_stride, int mode, int ctas_per_pe, const void **fn, dim3 *grid, dim3 *block,
                           unsigned *smem) {
   int rc;
-  if ((rc = need_started())) return rc;
+  if ((rc = need_collective())) return rc;
   const Runtime &r = rt();
   if ((op != NVSHMEMX_REQ_PUT && op != NVSHMEMX_REQ_GET) || dtype < 0 || dtype > NVSHMEMX_DT_DOUBLE ||
       mode < 0 || mode > NVSHMEMX_MODE_BULK || rounds < 1 || nsets < 1 || ctas_per_pe < 1 || r.npes < 2)
@@ -696,7 +708,7 @@ int nvshmemx_op_alltoall_host(int op, int dtype, size_t send_off, size_t recv_of
 static int halo_check(int px, int py, int pz, int n, size_t block_off, size_t ghost_off, size_t sig_off, int iters,
                       int *ctas_per_pe) {
   int rc;
-  if ((rc = need_started())) return rc;
+  if ((rc = need_collective())) return rc;
   const Runtime &r = rt();
   if (*ctas_per_pe == 0) *ctas_per_pe = max_ctas_per_pe((const void *)halo_kernel, 256, 0);
   if (px < 1 || py < 1 || pz < 1 || px * py * pz != r.npes || n < 1 || iters < 1 || *ctas_per_pe < 1)
@@ -748,7 +760,7 @@ int nvshmemx_op_halo_offload(int px, int py, int pz, int n, size_t block_off, si
 
 int nvshmemx_op_wait_test(size_t flag_off, int value, long long timeout_ns, int *out_status) {
   int rc;
-  if ((rc = need_started())) return rc;
+  if ((rc = need_collective())) return rc;
   const Runtime &r = rt();
   if (flag_off + 4 > r.heap_bytes || flag_off % 4) return fail(NVSHMEMX_ERR_INVALID, "wait_test: bad flag offset");
   int *d = (int *)g_out_buf.get(64);
@@ -761,7 +773,7 @@ int nvshmemx_op_wait_test(size_t flag_off, int value, long long timeout_ns, int 
 
 int nvshmemx_op_barrier_fault_test(int skip_pe, long long timeout_ns, int *out_status) {
   int rc;
-  if ((rc = need_started())) return rc;
+  if ((rc = need_collective())) return rc;
   const Runtime &r = rt();
   if (skip_pe < 0 || skip_pe >= r.npes || timeout_ns <= 0) return fail(NVSHMEMX_ERR_INVALID, "barrier_fault_test");
   int *d = (int *)g_out_buf.get(64);

@@ -108,6 +108,23 @@ def test_submit_end_to_end(shmem_factory):
     assert first_diff(heap_images(sh, npes, heap), om.heap) is None
 
 
+@pytest.mark.parametrize("n", [8191, 8192, 8193, 12345])
+def test_submit_at_the_split_point(shmem_factory, n):
+    """One piece below 8192 requests, two from 8192 on (the first a quarter
+    rounded down to whole 256-request blocks); same heaps either way."""
+    npes, heap = 8, 16 << 20
+    reqs = c4_batch(seed=50 + n, n=n, npes=npes, heap=heap, hi=8 << 10)
+    sh, om = setup(shmem_factory, npes, heap)
+    with sh.batch(len(reqs), int(reqs["bytes"].sum()), 256) as b:
+        st, _ = b.submit(reqs.copy())
+        assert st == 0
+        om.apply_requests(reqs)
+        assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+        chunks = b.stats()[0]
+        b.execute(1)
+        assert b.stats()[0] == chunks
+
+
 @pytest.mark.parametrize("cfg", [None, CONFIGS[0]], ids=["tma", "register"])
 def test_submit_pipelined_two_pieces(shmem_factory, cfg):
     """A submit of 8192 or more requests in a graph configuration runs in two
