@@ -364,6 +364,19 @@ __device__ __forceinline__ int halo_nbr(int pe, int d, int px, int py, int pz) {
 // device_barrier each iteration ends at the device barrier, without it the
 // caller follows the launch with nvshmem_barrier_all_offload (one iteration
 // per launch, the prototype's own structure).
+// The face rows are 2 KiB warp copies; they use the same checks and
+// translation as nvshmemx_putmem_warp, inlined with a 4-deep copy loop (the
+// public call is a shared out-of-line helper with a deeper loop tuned for
+// long copies, which costs this short-row kernel registers and a call).
+__device__ __forceinline__ void halo_row_put(const Cfg &c, double *dst_sym, const double *src, size_t bytes, int pe,
+                                             unsigned lane) {
+  if (!check_remote(c, dst_sym, bytes, pe) || !check_local(c, src, bytes)) return;
+  char *dst = xlate(c, dst_sym, pe);
+  const unsigned long long t0 = (c.trace && lane == 0) ? gtimer() : 0;
+  copy_coop<16, 4>(dst, reinterpret_cast<const char *>(src), bytes, lane, 32);
+  if (c.trace && lane == 0) trace_rec(c, NVSHMEMX_TRACE_PUT_INT, src, dst, bytes, pe, t0, gtimer());
+}
+
 __global__ void __launch_bounds__(256, 4) halo_kernel(Cfg c, int px, int py, int pz, int n, unsigned long long block_off,
                             unsigned long long ghost_off, unsigned long long sig_off, int iters, int it0,
                             int device_barrier) {
@@ -388,11 +401,11 @@ __global__ void __launch_bounds__(256, 4) halo_kernel(Cfg c, int px, int py, int
       } else if (d < 4) {
         // y face: row j is z=j, contiguous in x
         const int y0 = (d & 1) ? n - 1 : 0;
-        nvshmemx_putmem_warp(dst, blk + ((long long)j * n + y0) * n, (size_t)n * 8, nb);
+        halo_row_put(c, dst, blk + ((long long)j * n + y0) * n, (size_t)n * 8, nb, lane);
       } else {
         // z face: row j is y=j of plane z0
         const int z0 = (d & 1) ? n - 1 : 0;
-        nvshmemx_putmem_warp(dst, blk + ((long long)z0 * n + j) * n, (size_t)n * 8, nb);
+        halo_row_put(c, dst, blk + ((long long)z0 * n + j) * n, (size_t)n * 8, nb, lane);
       }
     }
     nvshmem_quiet();
