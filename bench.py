@@ -124,7 +124,7 @@ def barrier(dist):
 
 
 # ------------------------------------------------------------ CPU baseline
-def cpu_baseline(reqs, npes, heap, max_seconds=12.0):
+def cpu_baseline(reqs, npes, heap, max_seconds=12.0, warmup=1):
     from oracle import model as om  # the checker package; only this leg runs it
     if not os.path.exists(om.HOST_BENCH):
         om.build()
@@ -132,7 +132,8 @@ def cpu_baseline(reqs, npes, heap, max_seconds=12.0):
         f.write(reqs.tobytes())
         path = f.name
     try:
-        out = subprocess.run([om.HOST_BENCH, "batch", path, str(npes), str(heap), "1000000", str(max_seconds), "44"],
+        out = subprocess.run([om.HOST_BENCH, "batch", path, str(npes), str(heap), "1000000", str(max_seconds), "44",
+                              str(warmup)],
                              capture_output=True, text=True, timeout=600, check=True).stdout
     finally:
         os.unlink(path)
@@ -152,9 +153,9 @@ def run_reference(args, rank, world):
     from nvshmem_b200.traffic import c4_batch
     reqs = c4_batch(**C4)
     t0 = time.time()
-    cb = cpu_baseline(reqs, C4["npes"], C4["heap"], max_seconds=max(5.0, 2.0 * args.steps))
+    cb = cpu_baseline(reqs, C4["npes"], C4["heap"], max_seconds=max(5.0, 2.0 * args.steps), warmup=args.warmup)
     line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": cb["reps"],
-            "warmup": 1, "ms_per_step": round(cb["ms_per_step"], 4),
+            "warmup": args.warmup, "ms_per_step": round(cb["ms_per_step"], 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
             "data": "synthetic (seeded)", "impl": "reference",
             "config": {"workload": WORKLOAD, "parallelism": "one OS process per PE"},

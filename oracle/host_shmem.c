@@ -109,7 +109,8 @@ static void run_req(unsigned char *heap, size_t slice, const req_t *q) {
 /* Runs reps until max_reps or max_seconds; rank 0 reports seconds per rep
  * (between the barrier before and the barrier after the work, so the time
  * of the slowest rank). */
-static int cmd_batch(const char *file, int npes, size_t slice, int max_reps, double max_s, long long seed) {
+static int cmd_batch(const char *file, int npes, size_t slice, int max_reps, double max_s, long long seed,
+                     int warmup) {
   FILE *f = fopen(file, "rb");
   if (!f) {
     perror(file);
@@ -154,7 +155,8 @@ static int cmd_batch(const char *file, int npes, size_t slice, int max_reps, dou
   int reps = 0;
   double total = 0;
   const double start = now_s();
-  for (int rep = -1; rep < max_reps; ++rep) { /* rep -1: untimed warm-up */
+  if (warmup < 0) warmup = 0;
+  for (int rep = -warmup; rep < max_reps; ++rep) { /* negative reps: untimed warm-up */
     pthread_barrier_wait(&c->bar);
     const double t0 = now_s();
     for (int k = 0; k < nm; ++k) run_req(heap, slice, &reqs[mine[k]]);
@@ -279,7 +281,7 @@ static int cmd_barrier(int npes, int iters) {
 int main(int argc, char **argv) {
   if (argc >= 7 && strcmp(argv[1], "batch") == 0)
     return cmd_batch(argv[2], atoi(argv[3]), (size_t)atoll(argv[4]), atoi(argv[5]), atof(argv[6]),
-                     argc >= 8 ? atoll(argv[7]) : -1);
+                     argc >= 8 ? atoll(argv[7]) : -1, argc >= 9 ? atoi(argv[8]) : 1);
   if (argc >= 6 && strcmp(argv[1], "alltoall") == 0)
     return cmd_alltoall(atoi(argv[2]), (size_t)atoll(argv[3]), atoi(argv[4]), atof(argv[5]));
   if (argc >= 3 && strcmp(argv[1], "pingpong") == 0) return cmd_pingpong(atoi(argv[2]));
