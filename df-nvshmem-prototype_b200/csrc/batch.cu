@@ -69,17 +69,18 @@ __device__ __forceinline__ bool piece_may_run(BatchCtl *ctl, BatchCtl *sctl) {
 }
 
 // ------------------------------------------------------------------- plan
-// A batch is planned as one piece, or (pipelined submit) as two pieces, each
-// writing its items into its own region of the table, [ibase, cap_end), and
-// reporting errors, with request indices offset by `req_base`, in the first
-// piece's control block `sctl`.
+// A batch is planned as one piece, or (pipelined submit) as consecutive
+// pieces planned in order on one stream: piece k appends its items after
+// those of piece k-1 (`prev`) and reports errors, with request indices offset
+// by `req_base`, in its own control block `sctl`.
 __global__ void __launch_bounds__(256) batch_plan_kernel(Cfg c, const nvshmemx_request *__restrict__ reqs, int n,
                                                          unsigned chunk, WorkItem *__restrict__ items,
                                                          unsigned long long cap, BatchCtl *ctl, BatchCtl *sctl,
-                                                         unsigned long long ibase, int req_base) {
+                                                         const BatchCtl *prev, int req_base) {
   __shared__ unsigned warp_sums[8];
   __shared__ unsigned long long block_base;
   pdl_release_dependents();
+  const unsigned long long ibase = prev ? prev->item_base + prev->total_chunks : 0ull;
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->item_base = ibase;
   const int i = blockIdx.x * 256 + threadIdx.x;
   const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -727,8 +728,9 @@ struct nvshmemx_batch {
   int n = 0;
   nvshmemx_batch_config cfg{};
   cudaStream_t stream = nullptr;
-  cudaStream_t copy_stream = nullptr;  // pipelined submit: the second piece's copy
+  cudaStream_t copy_stream = nullptr;  // pipelined submit: copies and plans of the pieces
   cudaEvent_t ev_reset = nullptr, ev_copied = nullptr;
+  cudaEvent_t ev_piece[3] = {nullptr, nullptr, nullptr};  // piece k planned
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   int graph_n = -1;
@@ -737,22 +739,30 @@ struct nvshmemx_batch {
   Cfg graph_arena{};
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr, ev_plan0 = nullptr, ev_exec0 = nullptr, ev_exec1 = nullptr;
   bool timed_direct = false;  // ev_plan0/ev_exec0/ev_exec1 hold the last direct execution
-  bool last_split = false;    // the last execution was a two-piece submit
+  int last_pieces = 1;        // pieces of the last execution (pipelined submit: 2)
 };
 
-// Control block of the second piece of a pipelined submit: bytes 64..95 of
-// the batch's 128-byte control allocation (bytes 32..63 hold the streaming
-// generation, which must never be zeroed).
-static BatchCtl *second_ctl(nvshmemx_batch *b) {
-  return reinterpret_cast<BatchCtl *>(reinterpret_cast<char *>(b->d_ctl) + 64);
+// Control block of piece k of a pipelined submit: bytes 0..31, 64..95 and
+// 96..127 of the batch's 128-byte control allocation (bytes 32..63 hold the
+// streaming generation, which must never be zeroed).
+static BatchCtl *piece_ctl(nvshmemx_batch *b, int k) {
+  static const int off[3] = {0, 64, 96};
+  return reinterpret_cast<BatchCtl *>(reinterpret_cast<char *>(b->d_ctl) + off[k]);
 }
 
-// First-piece size of a pipelined submit: a quarter of the batch, in whole
-// 256-request plan blocks; 0 (one piece) below 8192 requests, where the copy
-// is too short to be worth hiding.
-static int split_point(int n) {
-  if (n < 8192) return 0;
-  return (n / 4) & ~255;
+// Pieces of a pipelined submit (ends[k] = end of piece k, in requests): one
+// below 8192 requests, where the copy is too short to be worth hiding, else
+// two, a quarter (in whole 256-request plan blocks) and the rest.  (Three
+// pieces, an eighth / three eighths / a half, measured 6 us slower on the
+// 100,000-request batch: each extra exec launch costs more than it hides.)
+static int split_pieces(int n, int ends[3]) {
+  if (n < 8192) {
+    ends[0] = n;
+    return 1;
+  }
+  ends[0] = (n / 4) & ~255;
+  ends[1] = n;
+  return 2;
 }
 
 static void drop_graph(nvshmemx_batch *b) {
@@ -791,14 +801,14 @@ static int enqueue_stream(nvshmemx_batch *b, bool with_events, const nvshmemx_re
 
 // Plan (parts & 1) and/or exec (parts & 2) of one piece of a batch (n
 // requests at `src`) on stream `st`, with the piece's control block `ctl`,
-// errors into `sctl`, and its items in [ibase, ibase + cap) of the table.
+// errors into `sctl`, and its items appended after those of `prev`.
 enum { kPlan = 1, kExec = 2 };
 static int enqueue_piece(nvshmemx_batch *b, bool with_events, const nvshmemx_request *src, int n, BatchCtl *ctl,
-                         BatchCtl *sctl, unsigned long long ibase, int req_base, cudaStream_t st, int parts) {
+                         BatchCtl *sctl, const BatchCtl *prev, int req_base, cudaStream_t st, int parts) {
   const Runtime &r = rt();
   const Cfg c = r.cfg;
   const nvshmemx_batch_config &k = b->cfg;
-  const unsigned long long cap_end = ibase + b->cap;
+  const unsigned long long cap_end = b->cap;
   ExecFn fn = pick_exec(k.vec_bytes, k.unroll);
   TmaFn tfn = k.tma_stages ? pick_tma(k.tma_stages) : nullptr;
   if (!fn || (k.tma_stages && !tfn))
@@ -808,7 +818,7 @@ static int enqueue_piece(nvshmemx_batch *b, bool with_events, const nvshmemx_req
   if (with_events) cudaEventRecord(b->ev_plan0, st);
   if ((parts & kPlan) && n > 0)
     batch_plan_kernel<<<(n + 255) / 256, 256, 0, st>>>(c, src, n, (unsigned)k.chunk_bytes, b->d_items, cap_end, ctl,
-                                                       sctl, ibase, req_base);
+                                                       sctl, prev, req_base);
   if (with_events) cudaEventRecord(b->ev_exec0, st);
   if (!(parts & kExec)) return check_cuda(cudaGetLastError(), "batch plan launch");
   const size_t smem = tfn ? tma_smem_bytes(k) : 0;
@@ -850,7 +860,7 @@ static int enqueue_piece(nvshmemx_batch *b, bool with_events, const nvshmemx_req
 static int enqueue_batch(nvshmemx_batch *b, bool with_events, const nvshmemx_request *src) {
   if (b->cfg.stream) return enqueue_stream(b, with_events, src);
   cudaMemsetAsync(b->d_ctl, 0, sizeof(BatchCtl), b->stream);
-  return enqueue_piece(b, with_events, src, b->n, b->d_ctl, b->d_ctl, 0, 0, b->stream, kPlan | kExec);
+  return enqueue_piece(b, with_events, src, b->n, b->d_ctl, b->d_ctl, nullptr, 0, b->stream, kPlan | kExec);
 }
 
 static int ensure_graph(nvshmemx_batch *b, const nvshmemx_request *src) {
@@ -914,7 +924,7 @@ int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes
   if (b->cfg.chunk_bytes < min_chunk_bytes) b->cfg.chunk_bytes = (min_chunk_bytes + 255) / 256 * 256;
   int rc = 0;
   if ((rc = check_cuda(cudaMalloc(&b->d_reqs, (size_t)max_requests * sizeof(nvshmemx_request)), "cudaMalloc(reqs)")) ||
-      (rc = check_cuda(cudaMalloc(&b->d_items, 2 * (size_t)b->cap * sizeof(WorkItem)), "cudaMalloc(items)")) ||
+      (rc = check_cuda(cudaMalloc(&b->d_items, (size_t)b->cap * sizeof(WorkItem)), "cudaMalloc(items)")) ||
       (rc = check_cuda(cudaMalloc(&b->d_ctl, 128), "cudaMalloc(ctl)")) ||
       (rc = check_cuda(cudaMallocHost(&b->h_reqs, (size_t)max_requests * sizeof(nvshmemx_request)),
                        "cudaMallocHost(reqs)")) ||
@@ -931,6 +941,7 @@ int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes
   cudaEventCreate(&b->ev_exec1);
   cudaEventCreateWithFlags(&b->ev_reset, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&b->ev_copied, cudaEventDisableTiming);
+  for (auto &e : b->ev_piece) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   void *hs = nullptr;
   if ((rc = check_cuda(cudaHostGetDevicePointer(&hs, b->h_status, 0), "cudaHostGetDevicePointer(status)"))) {
     nvshmemx_batch_destroy(b);
@@ -940,7 +951,7 @@ int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes
   // control block (BatchCtl or StreamCtl) and every work item's generation
   // tag start at zero; streaming generations start at 1
   cudaMemset(b->d_ctl, 0, 128);
-  cudaMemset(b->d_items, 0, 2 * (size_t)b->cap * sizeof(WorkItem));
+  cudaMemset(b->d_items, 0, (size_t)b->cap * sizeof(WorkItem));
   *out = b;
   return 0;
 }
@@ -955,7 +966,8 @@ int nvshmemx_batch_destroy(nvshmemx_batch *b) {
   if (b->d_ctl) cudaFree(b->d_ctl);
   if (b->h_reqs) cudaFreeHost(b->h_reqs);
   if (b->h_status) cudaFreeHost(b->h_status);
-  cudaEvent_t evs[] = {b->ev_start, b->ev_stop, b->ev_plan0, b->ev_exec0, b->ev_exec1, b->ev_reset, b->ev_copied};
+  cudaEvent_t evs[] = {b->ev_start,    b->ev_stop,     b->ev_plan0,    b->ev_exec0,   b->ev_exec1,
+                       b->ev_reset,    b->ev_copied,   b->ev_piece[0], b->ev_piece[1], b->ev_piece[2]};
   for (auto e : evs)
     if (e) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -995,7 +1007,7 @@ int nvshmemx_batch_execute(nvshmemx_batch *b, int reps, float *out_ms) {
   if (!b || reps < 1) return fail(NVSHMEMX_ERR_INVALID, "batch_execute: bad arguments");
   int rc;
   if ((rc = ensure_graph(b, b->d_reqs))) return rc;
-  b->last_split = false;
+  b->last_pieces = 1;
   cudaEventRecord(b->ev_start, b->stream);
   for (int i = 0; i < reps; ++i)
     if ((rc = check_cuda(cudaGraphLaunch(b->gexec, b->stream), "cudaGraphLaunch"))) return rc;
@@ -1014,37 +1026,45 @@ int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n
   if (!b || n < 0 || n > b->max_n || (n && !reqs)) return fail(NVSHMEMX_ERR_INVALID, "batch_submit: bad arguments");
   int rc;
   b->n = n;
-  const int n0 = b->cfg.stream ? 0 : split_point(n);
-  if (!n0 && (rc = ensure_graph(b, b->d_reqs))) return rc;
-  b->last_split = n0 > 0;
+  int ends[3];
+  const int pieces = b->cfg.stream ? 1 : split_pieces(n, ends);
+  if (pieces == 1 && (rc = ensure_graph(b, b->d_reqs))) return rc;
+  b->last_pieces = pieces;
   b->timed_direct = false;
   cudaEventRecord(b->ev_start, b->stream);
-  if (n0) {
-    // Two pieces, each with its own control block and region of the item
-    // table.  The batch's stream copies, plans and executes the first
-    // quarter; meanwhile the copy stream brings the rest and plans it (the
-    // plan kernel fits beside the running exec kernel); the second exec
-    // follows the first once that plan is done.
-    BatchCtl *c0 = b->d_ctl, *c1 = second_ctl(b);
-    if ((rc = check_cuda(cudaMemsetAsync(c0, 0, sizeof(BatchCtl), b->stream), "cudaMemsetAsync")) ||
-        (rc = check_cuda(cudaMemcpyAsync(b->d_reqs, reqs, (size_t)n0 * sizeof(nvshmemx_request),
-                                         cudaMemcpyHostToDevice, b->stream),
-                         "cudaMemcpyAsync(requests)")) ||
-        (rc = check_cuda(cudaEventRecord(b->ev_reset, b->stream), "cudaEventRecord")) ||
-        (rc = check_cuda(cudaStreamWaitEvent(b->copy_stream, b->ev_reset, 0), "cudaStreamWaitEvent")) ||
-        (rc = check_cuda(cudaMemsetAsync(c1, 0, sizeof(BatchCtl), b->copy_stream), "cudaMemsetAsync")) ||
-        (rc = check_cuda(cudaMemcpyAsync(b->d_reqs + n0, reqs + n0, (size_t)(n - n0) * sizeof(nvshmemx_request),
-                                         cudaMemcpyHostToDevice, b->copy_stream),
-                         "cudaMemcpyAsync(requests)")) ||
-        (rc = enqueue_piece(b, false, b->d_reqs + n0, n - n0, c1, c1, b->cap, n0, b->copy_stream, kPlan)) ||
-        (rc = check_cuda(cudaEventRecord(b->ev_copied, b->copy_stream), "cudaEventRecord")) ||
-        (rc = enqueue_piece(b, false, b->d_reqs, n0, c0, c0, 0, 0, b->stream, kPlan | kExec)) ||
-        (rc = check_cuda(cudaStreamWaitEvent(b->stream, b->ev_copied, 0), "cudaStreamWaitEvent")) ||
-        (rc = enqueue_piece(b, false, b->d_reqs + n0, n - n0, c1, c0, b->cap, n0, b->stream, kExec))) {
+  if (pieces > 1) {
+    // The copy stream copies and plans the pieces in order (each plan
+    // appends its items after the previous piece's); the batch's stream
+    // executes piece k once it is planned and piece k-1 has run.  Each piece
+    // has its own control block; the execs report into the first.
+    rc = check_cuda(cudaStreamWaitEvent(b->copy_stream, b->ev_start, 0), "cudaStreamWaitEvent");
+    if (!rc)
+      rc = check_cuda(cudaMemsetAsync(piece_ctl(b, 0), 0, sizeof(BatchCtl), b->copy_stream), "cudaMemsetAsync");
+    if (!rc)  // blocks 1 and 2 are contiguous (bytes 64..127)
+      rc = check_cuda(cudaMemsetAsync(piece_ctl(b, 1), 0, 2 * sizeof(BatchCtl), b->copy_stream), "cudaMemsetAsync");
+    for (int k = 0, at = 0; k < pieces && !rc; at = ends[k++]) {
+      const int m = ends[k] - at;
+      BatchCtl *ck = piece_ctl(b, k);
+      if ((rc = check_cuda(cudaMemcpyAsync(b->d_reqs + at, reqs + at, (size_t)m * sizeof(nvshmemx_request),
+                                           cudaMemcpyHostToDevice, b->copy_stream),
+                           "cudaMemcpyAsync(requests)")) ||
+          (rc = enqueue_piece(b, false, b->d_reqs + at, m, ck, ck, k ? piece_ctl(b, k - 1) : nullptr, at,
+                              b->copy_stream, kPlan)) ||
+          (rc = check_cuda(cudaEventRecord(b->ev_piece[k], b->copy_stream), "cudaEventRecord")))
+        break;
+    }
+    for (int k = 0, at = 0; k < pieces && !rc; at = ends[k++]) {
+      if ((rc = check_cuda(cudaStreamWaitEvent(b->stream, b->ev_piece[k], 0), "cudaStreamWaitEvent")) ||
+          (rc = enqueue_piece(b, false, b->d_reqs + at, ends[k] - at, piece_ctl(b, k), piece_ctl(b, 0), nullptr, at,
+                              b->stream, kExec)))
+        break;
+    }
+    if (rc) {
       cudaStreamSynchronize(b->copy_stream);
       cudaStreamSynchronize(b->stream);
       return rc;
     }
+    BatchCtl *c0 = piece_ctl(b, 0);
     // the status word reaches the host from a kernel that starts while the
     // last exec runs and writes as soon as it is done (no copy to schedule)
     cudaLaunchConfig_t lc = {};
@@ -1082,10 +1102,12 @@ int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n
 int nvshmemx_batch_last_stats(const nvshmemx_batch *b, unsigned long long *chunks, float *plan_ms, float *exec_ms) {
   if (!b) return NVSHMEMX_ERR_INVALID;
   if (chunks) {
-    BatchCtl h[3];  // bytes 0..95: first piece, (streaming state), second piece
+    BatchCtl h[4];  // bytes 0..127: piece 0, (streaming state), pieces 1 and 2
     if (cudaMemcpy(h, b->d_ctl, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess)
       return check_cuda(cudaGetLastError(), "batch_last_stats");
-    *chunks = h[0].total_chunks + (b->last_split ? h[2].total_chunks : 0ull);
+    *chunks = h[0].total_chunks;
+    if (b->last_pieces > 1) *chunks += h[2].total_chunks;
+    if (b->last_pieces > 2) *chunks += h[3].total_chunks;
   }
   float p = 0, e = 0;
   if (b->timed_direct) {
@@ -1105,7 +1127,7 @@ int nvshmemx_batch_execute_direct(nvshmemx_batch *b, int reps, float *out_ms, fl
   if (!b || reps < 1) return fail(NVSHMEMX_ERR_INVALID, "batch_execute_direct: bad arguments");
   int rc;
   float total = 0, exec = 0;
-  b->last_split = false;
+  b->last_pieces = 1;
   for (int i = 0; i < reps; ++i) {
     cudaEventRecord(b->ev_start, b->stream);
     if ((rc = enqueue_batch(b, true, b->d_reqs))) return rc;
@@ -1241,7 +1263,7 @@ extern "C" int nvshmemx_batch_execute_noalloc(const nvshmemx_request *d_reqs, in
   if ((rc = check_cuda(cudaMemsetAsync(ctl, 0, sizeof(BatchCtl), s), "cudaMemsetAsync(noalloc control)"))) return rc;
   if (n > 0)
     batch_plan_kernel<<<(n + 255) / 256, 256, 0, s>>>(r.cfg, d_reqs, n, (unsigned)k.chunk_bytes, items,
-                                                      kNoallocMaxItems, ctl, ctl, 0ull, 0);
+                                                      kNoallocMaxItems, ctl, ctl, nullptr, 0);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, k.threads, 0);
   if (per_sm < 1) per_sm = 1;

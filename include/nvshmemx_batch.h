@@ -64,8 +64,7 @@ typedef struct nvshmemx_batch nvshmemx_batch;
 /* Device buffers for up to max_requests requests moving up to
  * max_payload_bytes in total (sizes the chunk table for the smallest chunk
  * size a configuration may use, 256 bytes, unless min_chunk_bytes is larger;
- * the table is allocated twice over, one region per piece of a pipelined
- * submit, 32 bytes per chunk). */
+ * 32 bytes per chunk). */
 int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes, int min_chunk_bytes,
                           nvshmemx_batch **out);
 int nvshmemx_batch_destroy(nvshmemx_batch *b);
@@ -89,9 +88,9 @@ int nvshmemx_batch_execute(nvshmemx_batch *b, int reps, float *out_ms);
  * *out_status receives the status (0 = every request done), *out_ms the
  * device time of the whole sequence.  With a graph configuration (stream 0)
  * the copy precedes the plan and exec kernels on the batch's stream; from
- * 8192 requests on, the batch runs as two pieces: the first quarter (in
- * whole 256-request blocks) is copied, planned and executed while a second
- * stream copies and plans the rest, which executes after the first, and a
+ * 8192 requests on, the batch runs as two pieces: a second stream copies
+ * and plans the first quarter (in whole 256-request blocks), then the rest,
+ * while the batch's stream executes each piece once it is planned, and a
  * one-thread kernel writes the status word into pinned host memory.  An
  * invalid request in the second piece is reported after the first piece has
  * run (with one piece, nothing runs).  In stream mode the copy precedes the

@@ -108,11 +108,16 @@ def test_submit_end_to_end(shmem_factory):
     assert first_diff(heap_images(sh, npes, heap), om.heap) is None
 
 
-@pytest.mark.parametrize("n", [8191, 8192, 8193, 12345])
+def split_ends(n):
+    """Piece boundaries of a pipelined submit, as the library splits."""
+    return [n] if n < 8192 else [(n // 4) & ~255, n]
+
+
+@pytest.mark.parametrize("n", [8191, 8192, 8193, 12345, 40000])
 def test_submit_at_the_split_point(shmem_factory, n):
     """One piece below 8192 requests, two from 8192 on (the first a quarter
-    rounded down to whole 256-request blocks); same heaps either way."""
-    npes, heap = 8, 16 << 20
+    in whole 256-request blocks); same heaps either way."""
+    npes, heap = 8, 32 << 20
     reqs = c4_batch(seed=50 + n, n=n, npes=npes, heap=heap, hi=8 << 10)
     sh, om = setup(shmem_factory, npes, heap)
     with sh.batch(len(reqs), int(reqs["bytes"].sum()), 256) as b:
@@ -125,13 +130,14 @@ def test_submit_at_the_split_point(shmem_factory, n):
         assert b.stats()[0] == chunks
 
 
+@pytest.mark.parametrize("n", [20000, 40000])
 @pytest.mark.parametrize("cfg", [None, CONFIGS[0]], ids=["tma", "register"])
-def test_submit_pipelined_two_pieces(shmem_factory, cfg):
-    """A submit of 8192 or more requests in a graph configuration runs in two
-    pieces: the first quarter executes while the rest is copied, and the
-    second piece's chunks are appended after the first's."""
-    npes, heap = 16, 16 << 20
-    reqs = c4_batch(seed=48, n=20000, npes=npes, heap=heap, hi=16 << 10)
+def test_submit_pipelined(shmem_factory, cfg, n):
+    """A submit of 8192 or more requests in a graph configuration runs in
+    pieces: each executes while the next is copied and planned (appending its
+    chunks after the previous piece's)."""
+    npes, heap = 16, 32 << 20
+    reqs = c4_batch(seed=48, n=n, npes=npes, heap=heap, hi=16 << 10)
     sh, om = setup(shmem_factory, npes, heap)
     with sh.batch(len(reqs), int(reqs["bytes"].sum()), 256) as b:
         if cfg:
@@ -147,9 +153,9 @@ def test_submit_pipelined_two_pieces(shmem_factory, cfg):
         b.execute(1)
         assert b.stats()[0] == chunks
         assert first_diff(heap_images(sh, npes, heap), om.heap) is None
-        # a bad request in the second piece: the first piece has run, the
-        # second has not
-        n0 = (len(reqs) // 4) & ~255
+        # a bad request in the last piece: the pieces before it have run, the
+        # last has not
+        n0 = split_ends(len(reqs))[-2]
         for pe in range(npes):
             sh.fill_random(pe, 0, heap, 8)
         om2 = Model(npes, heap)
