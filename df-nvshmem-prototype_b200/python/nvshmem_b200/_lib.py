@@ -86,6 +86,7 @@ _SIGS = {
     "nvshmem_ptr": (c_void_p, [c_void_p, c_int]),
     # nvshmemx.h host
     "nvshmemx_init_attr": (c_int, [c_int, c_size_t]), "nvshmemx_finalize": (c_int, []),
+    "nvshmemx_init_process": (c_int, [c_int, c_int, c_size_t, c_char_p]),
     "nvshmemx_is_started": (c_int, []), "nvshmemx_status": (c_int, []),
     "nvshmemx_status_detail": (c_longlong, []),
     "nvshmemx_set_error_mode": (None, [c_int]), "nvshmemx_get_error_mode": (c_int, []),

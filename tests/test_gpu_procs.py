@@ -64,3 +64,35 @@ def test_departed_process_fails_the_barrier(tmp_path):
     codes = launch([exe, "depart", str(tmp_path)], 3, heap=4 << 20, timeout=240, stop_on_failure=False,
                    env=dict(os.environ, NVSHMEM_HOST_BARRIER_TIMEOUT_S="3"))
     assert codes == [3, 0, 3], codes
+
+
+def test_process_start_failures_leave_the_library_usable(tmp_path):
+    """nvshmemx_init_process fails cleanly -- an unusable rendezvous
+    directory, or a peer that never arrives (bounded by the host timeout) --
+    and a one-process start works afterwards in the same process."""
+    import subprocess
+    import sys
+    pkg = os.path.join(REPO, "df-nvshmem-prototype_b200", "python")
+    code = "\n".join([
+        "import os, sys, time",
+        f"sys.path.insert(0, {pkg!r})",
+        "from nvshmem_b200 import _lib as L",
+        "lib = L.lib",
+        "lib.nvshmemx_set_error_mode(1)",
+        "rc1 = lib.nvshmemx_init_process(0, 2, 1 << 20, b'/nonexistent/rendezvous')",
+        "assert not lib.nvshmemx_is_started()",
+        "t0 = time.time()",
+        f"rc2 = lib.nvshmemx_init_process(0, 2, 1 << 20, {str(tmp_path).encode()!r})",
+        "dt = time.time() - t0",
+        "assert not lib.nvshmemx_is_started()",
+        "lib.nvshmemx_status()",
+        "rc3 = lib.nvshmemx_init_attr(2, 1 << 20)",
+        "assert lib.nvshmemx_is_started() and lib.nvshmemx_finalize() == 0",
+        "print(rc1, rc2, rc3, round(dt, 1))",
+    ])
+    env = dict(os.environ, NVSHMEM_HOST_BARRIER_TIMEOUT_S="2")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    rc1, rc2, rc3, dt = r.stdout.split()
+    assert int(rc1) != 0 and int(rc2) != 0 and int(rc3) == 0
+    assert 1.5 <= float(dt) <= 30  # the missing peer is given up on after the timeout
