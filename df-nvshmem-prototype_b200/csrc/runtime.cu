@@ -862,6 +862,8 @@ int nvshmemx_trace_write_csv(const char *prefix) {
   std::string pre = prefix ? prefix : ("nvshmem_processed_tracefile_" + std::to_string((long)getpid()));
   std::vector<nvshmemx_trace_record> recs(r.trace_cap);
   for (int pe = 0; pe < r.npes; ++pe) {
+    // one process per PE: each process records and writes its own PE only
+    if (proc_mode() && pe != proc_pe()) continue;
     long long dropped = 0;
     long long n = nvshmemx_trace_read(pe, recs.data(), recs.size(), &dropped);
     if (n < 0) return fail(NVSHMEMX_ERR_CUDA, "trace read failed");
