@@ -4,7 +4,7 @@ in csrc/tuner.cu does the timing) and keeps the measured table as JSON.
   python -m nvshmem_b200.tune [--workload c4] [--reps 5] [--out PATH]
 
 The table ({"key", "results": [...], "best": {...}}) is what bench.py loads,
-what the learned picker falls back to, and what judges the picker's regret.
+what the learned picker falls back to, and the yardstick for the picker's regret.
 """
 from __future__ import annotations
 

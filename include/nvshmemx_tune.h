@@ -7,7 +7,7 @@
  * chosen by measuring candidates on the device: each candidate runs the
  * uploaded batch `reps` times with L2 flushed before every run, timed with
  * CUDA events; the median decides.  The measured table is also what the
- * learned picker falls back to and what judges its regret.
+ * learned picker falls back to and the yardstick for its regret.
  */
 #ifndef NVSHMEM_B200_NVSHMEMX_TUNE_H_
 #define NVSHMEM_B200_NVSHMEMX_TUNE_H_
