@@ -279,6 +279,11 @@ static int init_impl(int npes, size_t heap, int proc_pe = -1, const char *dir = 
   if (to) r.wait_timeout_ns = atoll(to);
 
   int rc;
+  // one process per PE may put its PE on a device of its own (the launcher's
+  // --devices); the slices of PEs on other devices are then mapped over the
+  // GPUs' peer links with the same exchanged handles
+  const char *dv = getenv("NVSHMEM_DEVICE");
+  if (proc_pe >= 0 && dv && (rc = check_cuda(cudaSetDevice(atoi(dv)), "cudaSetDevice(NVSHMEM_DEVICE)"))) return rc;
   if ((rc = check_cuda(cudaFree(0), "cudaFree(0)"))) return rc;  // create the context
   if ((rc = check_cuda(cudaGetDevice(&r.device), "cudaGetDevice"))) return rc;
   if ((rc = load_driver())) return rc;

@@ -1,7 +1,7 @@
 """Starts one process per PE for the library's process-per-PE mode, the
 stand-in for the prototype's ``mpirun -np N ./app`` (no MPI is needed).
 
-    python -m nvshmem_b200.launch -n 4 [--heap BYTES] [--timeout S] -- ./app args
+    python -m nvshmem_b200.launch -n 4 [--heap BYTES] [--timeout S] [--devices D] -- ./app args
 
 Every process gets NVSHMEM_NPES, NVSHMEM_PROCESS_PE and NVSHMEM_RENDEZVOUS
 (a fresh private directory where the processes exchange their slices' VMM
@@ -21,10 +21,12 @@ import time
 
 
 def launch(cmd: list[str], npes: int, heap: int | None = None, timeout: float | None = None,
-           env: dict | None = None, cwd: str | None = None, stop_on_failure: bool = True) -> list[int]:
+           env: dict | None = None, cwd: str | None = None, stop_on_failure: bool = True,
+           devices: int | None = None) -> list[int]:
     """Runs `cmd` as `npes` PE processes; returns their exit statuses (a PE
     stopped because another failed -- with stop_on_failure -- or because the
-    timeout passed reports -9)."""
+    timeout passed reports -9).  With `devices`, PE k runs on device
+    k % devices (NVSHMEM_DEVICE)."""
     if npes < 1:
         raise ValueError("npes must be at least 1")
     rdv = tempfile.mkdtemp(prefix="nvshm-")
@@ -35,6 +37,8 @@ def launch(cmd: list[str], npes: int, heap: int | None = None, timeout: float | 
             e.update(NVSHMEM_NPES=str(npes), NVSHMEM_PROCESS_PE=str(pe), NVSHMEM_RENDEZVOUS=rdv)
             if heap:
                 e["NVSHMEM_HEAP_SIZE"] = str(heap)
+            if devices:
+                e["NVSHMEM_DEVICE"] = str(pe % devices)
             procs.append(subprocess.Popen(cmd, env=e, cwd=cwd))
         deadline = None if timeout is None else time.monotonic() + timeout
         codes: list[int | None] = [None] * npes
@@ -66,12 +70,14 @@ def main() -> int:
     ap.add_argument("-n", "--npes", type=int, required=True)
     ap.add_argument("--heap", type=int, default=None, help="bytes per PE (NVSHMEM_HEAP_SIZE)")
     ap.add_argument("--timeout", type=float, default=None, help="seconds before every PE is stopped")
+    ap.add_argument("--devices", type=int, default=None,
+                    help="spread the PEs over this many GPUs (PE k on device k %% devices)")
     ap.add_argument("cmd", nargs=argparse.REMAINDER)
     a = ap.parse_args()
     cmd = a.cmd[1:] if a.cmd and a.cmd[0] == "--" else a.cmd
     if not cmd:
         ap.error("no command")
-    codes = launch(cmd, a.npes, a.heap, a.timeout)
+    codes = launch(cmd, a.npes, a.heap, a.timeout, devices=a.devices)
     return next((c for c in codes if c != 0), 0)
 
 

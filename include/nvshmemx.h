@@ -91,7 +91,8 @@ int nvshmemx_init_attr(int npes, size_t heap_bytes_per_pe);
  * same (kernels of different processes cannot wait for each other on one GPU,
  * so device-side waits on another process's data are not supported).
  * nvstart_pes enters this mode when NVSHMEM_PROCESS_PE and
- * NVSHMEM_RENDEZVOUS are set (python -m nvshmem_b200.launch sets them). */
+ * NVSHMEM_RENDEZVOUS are set (python -m nvshmem_b200.launch sets them);
+ * NVSHMEM_DEVICE, when set, selects this process's device first. */
 int nvshmemx_init_process(int pe, int npes, size_t heap_bytes_per_pe, const char *rendezvous_dir);
 /* nvstop_pes with a status code. */
 int nvshmemx_finalize(void);

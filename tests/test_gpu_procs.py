@@ -35,12 +35,20 @@ def pattern(pe, n):
     return ((pe * 2654435761 + i * 40503 + 7) & 0xFFFFFFFF).astype(np.uint32)
 
 
-@pytest.mark.parametrize("npes", [2, 4])
-def test_processes_exchange_blocks(tmp_path, npes):
+def visible_devices():
+    import torch
+    return torch.cuda.device_count()
+
+
+@pytest.mark.parametrize("npes,spread", [(2, False), (4, False), (4, True)])
+def test_processes_exchange_blocks(tmp_path, npes, spread):
+    """spread: the launcher's --devices over every visible GPU (PE k on
+    device k % count; on a one-GPU box every PE names device 0)."""
     exe = build(tmp_path)
     heap = 4 << 20
     codes = launch([exe, "exchange", str(tmp_path)], npes, heap=heap, timeout=240,
-                   env=dict(os.environ, NVSHMEM_HOST_BARRIER_TIMEOUT_S="60"))
+                   env=dict(os.environ, NVSHMEM_HOST_BARRIER_TIMEOUT_S="60"),
+                   devices=visible_devices() if spread else None)
     assert codes == [0] * npes, codes
     rows = [list(map(int, (tmp_path / f"pe{pe}.txt").read_text().split())) for pe in range(npes)]
     assert sorted(r[0] for r in rows) == list(range(npes))
