@@ -8,7 +8,7 @@ import pytest
 from nvshmem_b200 import (DT_DOUBLE, DT_FLOAT, DT_INT, ERR_TIMEOUT, MODE_BLOCK,
                           MODE_BULK, MODE_THREAD, MODE_WARP, REQ_GET, REQ_PUT)
 from nvshmem_b200.traffic import c3_block
-from oracle.model import Model
+from oracle.model import Model, checksum
 from _util import first_diff, heap_images
 
 pytestmark = pytest.mark.gpu
@@ -109,6 +109,36 @@ def test_alltoall_large_on_device_compare(shmem_factory):
             if p == q:
                 continue
             assert sh.compare(q, npes * nbytes + p * nbytes, p, q * nbytes, nbytes) == 0
+
+
+def test_alltoall_every_c2_size(shmem_factory):
+    """The whole C2 sweep, 26 message sizes from 8 B to 256 MiB (int, float
+    and double in turn), put and get through the TMA form: after each call
+    PE q's receive slot p holds exactly PE p's send slot q, and no other byte
+    of the receive area changed."""
+    from nvshmem_b200 import DT_DOUBLE
+    from nvshmem_b200.traffic import c2_sizes
+    npes, top = 8, 256 << 20
+    heap = 2 * npes * top + (2 << 20)
+    sh = shmem_factory(npes, heap)
+    dts = (DT_INT, DT_FLOAT, DT_DOUBLE)
+    for i, nbytes in enumerate(c2_sizes()):
+        dt = dts[i % 3]
+        for op in (REQ_PUT, REQ_GET):
+            recv = npes * nbytes
+            for pe in range(npes):
+                sh.fill_random(pe, 0, npes * nbytes, 100 + i)
+                sh.memset(pe, recv, 0, npes * nbytes + 64)
+            sh.alltoall(op, dt, 0, recv, nbytes, mode=MODE_BULK, ctas_per_pe=18)
+            assert sh.status() == 0
+            zero = checksum(np.zeros(nbytes, np.uint8))
+            for p in range(npes):
+                for q in range(npes):
+                    if p != q:
+                        assert sh.compare(q, recv + p * nbytes, p, q * nbytes, nbytes) == 0, (nbytes, op, p, q)
+                # its own slot and the 64 bytes past the area stay zero
+                assert sh.checksum(p, recv + p * nbytes, nbytes) == zero, (nbytes, op, p)
+                assert sh.checksum(p, recv + npes * nbytes, 64) == checksum(np.zeros(64, np.uint8))
 
 
 @pytest.mark.parametrize("offload", [False, True], ids=["persistent", "offload_barrier"])
