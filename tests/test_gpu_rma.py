@@ -63,6 +63,30 @@ def test_put_get_lengths(shmem_factory, dtype, nelems):
     assert first_diff(heap_images(sh, 2, heap), om.heap) is None
 
 
+@pytest.mark.parametrize("mode", MODES)
+def test_long_copies_every_alignment(shmem_factory, mode):
+    """Copies long enough for the thread and warp forms' L2 prefetch (32 KiB
+    and up, and just below), at every 4-byte relative alignment of source and
+    destination, put and get, all in one launch: bit-exact against the
+    oracle (the prefetch is a hint; it must never change a byte)."""
+    heap = 32 << 20
+    sh, om = start(shmem_factory, 2, heap=heap)
+    rows, cur = [], heap // 4
+    for nbytes in (32768 - 4, 32768, 65536 + 12, 1 << 20, (1 << 20) + 4):
+        for mis in (0, 4, 8, 12):
+            for op, (sp, dp) in ((REQ_PUT, (0, 1)), (REQ_GET, (1, 0))):
+                cur = (cur + 63) // 64 * 64
+                rows.append(dict(src_off=64 + 4 * (len(rows) % 4), dst_off=cur + mis + 4 * (len(rows) % 4),
+                                 bytes=nbytes, src_pe=sp, dst_pe=dp, op=op, dtype=DT_INT))
+                cur += nbytes + 64 + 16
+    assert cur < heap
+    reqs = requests(rows)
+    sh.exec_requests(reqs, mode)
+    assert sh.status() == 0
+    om.apply_requests(reqs)
+    assert first_diff(heap_images(sh, 2, heap), om.heap) is None
+
+
 def test_p_g_all_types(shmem_factory):
     sh, om = start(shmem_factory, 2)
     rows = []
