@@ -322,7 +322,11 @@ __device__ __forceinline__ BulkRing make_ring(void *smem, unsigned smem_bytes, u
 }
 
 // Single-thread bulk pipeline for a 16-byte aligned body (dst, src 16-aligned,
-// bytes a multiple of 16): loads run up to `stages` ahead of the stores.
+// bytes a multiple of 16): loads run up to `stages` - 1 ahead of the stores,
+// and a stage is reloaded one store later than it could be, so the issuing
+// thread never waits on the store it has just started (measured against
+// reloading the stage of the newest store: one CTA's 1 MiB put 51 -> 60 GB/s,
+// the 16 MiB all-to-all 6350 -> 6565 GB/s with 6 stages).
 // Returns false if an mbarrier wait passed `deadline` (the copy is then
 // incomplete; every issued store is still drained before returning).
 __device__ __forceinline__ bool bulk_copy_1t(const BulkRing &ring, char *dst, const char *src,
@@ -350,12 +354,15 @@ __device__ __forceinline__ bool bulk_copy_1t(const BulkRing &ring, char *dst, co
     unsigned len = (unsigned)((bytes - c * SB) < SB ? (bytes - c * SB) : SB);
     bulk_s2g(dst + c * SB, ring.buf + (size_t)s * SB, len);
     bulk_commit();
-    const unsigned long long n = c + S;
-    if (n < nch) {
-      bulk_wait_read0();
+    // refill the stage the previous store read, not this one: that store has
+    // had a whole load wait to finish reading, while this one just started
+    const unsigned long long n = c - 1 + S;
+    if (c >= 1 && n < nch) {
+      asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+      const unsigned ps = (unsigned)((c - 1) % S);
       unsigned nlen = (unsigned)((bytes - n * SB) < SB ? (bytes - n * SB) : SB);
-      mbar_expect_tx(ring.mbar + s, nlen);
-      bulk_g2s(ring.buf + (size_t)s * SB, src + n * SB, nlen, ring.mbar + s);
+      mbar_expect_tx(ring.mbar + ps, nlen);
+      bulk_g2s(ring.buf + (size_t)ps * SB, src + n * SB, nlen, ring.mbar + ps);
     }
   }
   bulk_wait_all();
@@ -376,7 +383,7 @@ __device__ __forceinline__ void bulk_copy_block(const Cfg &c, char *dst, const c
                                                 unsigned long long bytes, void *smem,
                                                 unsigned smem_bytes) {
   const unsigned r = block_rank(), n = block_size();
-  BulkRing ring = make_ring(smem, smem_bytes, 4);
+  BulkRing ring = make_ring(smem, smem_bytes, 6);
   if ((((uintptr_t)dst ^ (uintptr_t)src) & 15) != 0 || ring.stage_bytes < 1024 || bytes < 4096 ||
       n < 64) {
     copy_coop<16, 4>(dst, src, bytes, r, n);

@@ -459,8 +459,8 @@ static int last_launch(const char *what) {
   return check_cuda(cudaGetLastError(), what);
 }
 
-// Shared memory for the CTA-wide TMA copies: a 4 x 16 KiB ring plus 128
-// bytes of mbarriers (three CTAs fit an SM).
+// Shared memory for the CTA-wide TMA copies: a 64 KiB ring (six stages)
+// plus 128 bytes of mbarriers (three CTAs fit an SM).
 static const unsigned kBulkSmem = 4 * 16384 + 128;
 
 namespace nvshm {

@@ -202,9 +202,12 @@ __device__ void nvshmemx_float_get_block(float *target, float *source, int len, 
 __device__ void nvshmemx_double_get_block(double *target, double *source, int len, int pe);
 
 /* Block-cooperative copy staged through shared memory with cp.async.bulk
- * (global -> shared -> global, mbarrier-tracked ring of stages).  `smem` must
- * be 128-byte aligned shared memory of `smem_bytes` >= 4 KiB; unaligned heads
- * and tails are copied by the generic path.  All threads of the block call. */
+ * (global -> shared -> global, mbarrier-tracked ring of six stages).  `smem`
+ * must be 128-byte aligned shared memory; with `smem_bytes` below 6272 (six
+ * stages of 1 KiB plus 128 bytes of mbarriers) the copy takes the generic
+ * path, and 64 KiB is what the library's own launches give it.  Unaligned
+ * heads and tails are copied by the generic path.  All threads of the block
+ * call. */
 __device__ void nvshmemx_putmem_bulk_block(void *target, const void *source, size_t bytes,
                                            int pe, void *smem, unsigned int smem_bytes);
 __device__ void nvshmemx_getmem_bulk_block(void *target, const void *source, size_t bytes,
