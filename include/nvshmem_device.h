@@ -10,7 +10,9 @@
  *    PE `pe`'s slice as  arena + pe*stride + ((addr - arena) & (stride-1)).
  *  - the other pointer of put/get is used as given (a local device pointer).
  *  - put/get copy `len` ELEMENTS; the calling thread copies all of them (the
- *    warp/block/bulk cooperative forms are in nvshmemx.h).
+ *    warp/block/bulk cooperative forms are in nvshmemx.h).  From 32 KiB on,
+ *    the thread also has the TMA unit prefetch its source into L2 16 KiB
+ *    ahead of its loads (a hint: the bytes copied are the same).
  *  - nvshmem_quiet orders all earlier stores of the calling thread before its
  *    later ones at GPU scope (all PEs share one GPU, so L2 is the coherence
  *    point; the prototype needed the system-scope fence of PCIe P2P).
