@@ -125,3 +125,29 @@ def test_every_device_function_links_with_device_lto(tmp_path):
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-3000:]
     assert out.exists()
+
+
+def _reference_readable():
+    r = subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle", "ref_build"), "have-ref"],
+                       capture_output=True, text=True)
+    return r.returncode == 0
+
+
+@pytest.mark.skipif(subprocess.run(["which", "nvcc"], capture_output=True).returncode != 0, reason="no nvcc")
+@pytest.mark.skipif(not _reference_readable(), reason="the reference sources are not on this machine")
+def test_reference_microbenchmarks_build_unchanged_against_this_library():
+    """The prototype's two microbenchmarks (microbench/shmem_latency.cu and
+    microbench/shmem_sync_latency.cu), compiled as they are with this
+    library's nvshmem.h / nvshmem_device.h and linked with its libnvshmem.a
+    (oracle/ref_build, target `compat`; the project's MPI subset stands in for
+    MPI).  They are not run: their two ranks spin on each other from separate
+    processes, which one GPU does not guarantee to run together."""
+    ref_build = os.path.join(REPO, "oracle", "ref_build")
+    deps = subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-rdc=true", "-I", INC, "-I",
+                           ref_build, "-M", "-x", "cu", "-"], input='#include "nvshmem.h"\n#include "nvshmem_device.h"\n',
+                          capture_output=True, text=True, timeout=300)
+    assert deps.returncode == 0 and os.path.join(INC, "nvshmem.h") in deps.stdout
+    r = subprocess.run(["make", "-B", "-C", ref_build, "compat"], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-3000:]
+    for name in ("compat_shmem_latency", "compat_shmem_sync_latency"):
+        assert os.path.exists(os.path.join(REPO, "oracle", "_ref", name))
