@@ -633,12 +633,23 @@ int nvshmemx_op_offload_barrier(int iters, double *out_us_per_call) {
 
 // Validates the arguments and picks the kernel, grid and block of an
 // all-to-all in `mode`.
+// CTAs per PE for an operation called with 0: NVSHMEM_CTAS_PER_PE when it is
+// set to a positive count, else the operation's own choice `fallback`.
+static int default_ctas_per_pe(int fallback) {
+  const char *v = getenv("NVSHMEM_CTAS_PER_PE");
+  const int k = v ? atoi(v) : 0;
+  return k > 0 ? k : fallback;
+}
+
 static int alltoall_setup(int op, int dtype, size_t send_off, size_t recv_off, size_t bytes, int rounds, int nsets,
                           size_t set_stride, int mode, int ctas_per_pe, const void **fn, dim3 *grid, dim3 *block,
                           unsigned *smem) {
   int rc;
   if ((rc = need_collective())) return rc;
   const Runtime &r = rt();
+  // 0: one CTA per PE per 1/npes of the SMs (18 for 8 PEs on 148 SMs: one
+  // ring-driving CTA per SM measured fastest from 4 MiB messages on)
+  if (ctas_per_pe == 0) ctas_per_pe = default_ctas_per_pe(r.sm_count / r.npes > 0 ? r.sm_count / r.npes : 1);
   if ((op != NVSHMEMX_REQ_PUT && op != NVSHMEMX_REQ_GET) || dtype < 0 || dtype > NVSHMEMX_DT_DOUBLE ||
       mode < 0 || mode > NVSHMEMX_MODE_BULK || rounds < 1 || nsets < 1 || ctas_per_pe < 1 || r.npes < 2)
     return fail(NVSHMEMX_ERR_INVALID, "alltoall: bad arguments");
@@ -716,14 +727,14 @@ int nvshmemx_op_alltoall_host(int op, int dtype, size_t send_off, size_t recv_of
   return check_cuda(cudaDeviceSynchronize(), "alltoall_host");
 }
 
-// ctas_per_pe 0: as many CTAs per PE as stay co-resident (the exchange is
-// latency-bound, so more warps in flight help).
+// ctas_per_pe 0: NVSHMEM_CTAS_PER_PE if set, else as many CTAs per PE as stay
+// co-resident (the exchange is latency-bound, so more warps in flight help).
 static int halo_check(int px, int py, int pz, int n, size_t block_off, size_t ghost_off, size_t sig_off, int iters,
                       int *ctas_per_pe) {
   int rc;
   if ((rc = need_collective())) return rc;
   const Runtime &r = rt();
-  if (*ctas_per_pe == 0) *ctas_per_pe = max_ctas_per_pe((const void *)halo_kernel, 256, 0);
+  if (*ctas_per_pe == 0) *ctas_per_pe = default_ctas_per_pe(max_ctas_per_pe((const void *)halo_kernel, 256, 0));
   if (px < 1 || py < 1 || pz < 1 || px * py * pz != r.npes || n < 1 || iters < 1 || *ctas_per_pe < 1)
     return fail(NVSHMEMX_ERR_INVALID, "halo: grid %dx%dx%d does not match %d PEs", px, py, pz, r.npes);
   const size_t nn = (size_t)n;

@@ -105,7 +105,8 @@ int nvshmemx_op_offload_barrier(int iters, double *out_us_per_call);
  * nvshmem_quiet and the device barrier.  Round r uses buffer set r % nsets,
  * set s at send_off + s*set_stride / recv_off + s*set_stride, so the working
  * set can exceed L2.  mode: NVSHMEMX_MODE_* (THREAD = one thread per message
- * through nvshmem_{T}_put/get).  dtype selects the typed call for THREAD. */
+ * through nvshmem_{T}_put/get).  dtype selects the typed call for THREAD.
+ * ctas_per_pe 0: NVSHMEM_CTAS_PER_PE if set, else SMs / npes. */
 int nvshmemx_op_alltoall(int op, int dtype, size_t send_off, size_t recv_off, size_t bytes,
                          int rounds, int nsets, size_t set_stride, int mode, int ctas_per_pe,
                          float *out_ms);
@@ -124,8 +125,9 @@ int nvshmemx_op_alltoall_host(int op, int dtype, size_t send_off, size_t recv_of
  * receiver gets from its -x neighbour goes to its -x ghost), then quiets,
  * sets the neighbour's signal (int at sig_off + 4*face) to it+1 with
  * nvshmem_int_p, waits for its own 6 signals with nvshmem_int_wait_until,
- * and meets the others at the device barrier.  ctas_per_pe 0 launches as
- * many CTAs per PE as stay co-resident. */
+ * and meets the others at the device barrier.  ctas_per_pe 0 launches
+ * NVSHMEM_CTAS_PER_PE CTAs per PE if that is set, else as many as stay
+ * co-resident. */
 int nvshmemx_op_halo(int px, int py, int pz, int n, size_t block_off, size_t ghost_off,
                      size_t sig_off, int iters, int ctas_per_pe, float *out_ms);
 /* The same exchange in the prototype's own structure: one collective launch

@@ -111,6 +111,27 @@ def test_alltoall_large_on_device_compare(shmem_factory):
             assert sh.compare(q, npes * nbytes + p * nbytes, p, q * nbytes, nbytes) == 0
 
 
+@pytest.mark.parametrize("env", [None, "5"], ids=["default", "NVSHMEM_CTAS_PER_PE=5"])
+def test_ctas_per_pe_zero_picks_a_default(shmem_factory, monkeypatch, env):
+    """ctas_per_pe 0: NVSHMEM_CTAS_PER_PE when set, else the operation's own
+    default; the heaps match the oracle either way."""
+    if env:
+        monkeypatch.setenv("NVSHMEM_CTAS_PER_PE", env)
+    else:
+        monkeypatch.delenv("NVSHMEM_CTAS_PER_PE", raising=False)
+    npes, heap = 8, 4 << 20
+    sh = shmem_factory(npes, heap)
+    om = Model(npes, heap)
+    for pe in range(npes):
+        sh.fill_random(pe, 0, heap, 3)
+        om.fill_random(pe, 0, heap, 3)
+    for mode in (MODE_BLOCK, MODE_BULK):
+        sh.alltoall(REQ_PUT, DT_FLOAT, 0, heap // 2, 65536 + 4, rounds=2, mode=mode, ctas_per_pe=0)
+        om.alltoall(0, 0, heap // 2, 65536 + 4, rounds=2)
+    assert sh.status() == 0
+    assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+
+
 def test_alltoall_every_c2_size(shmem_factory):
     """The whole C2 sweep, 26 message sizes from 8 B to 256 MiB (int, float
     and double in turn), put and get through the TMA form: after each call
