@@ -292,8 +292,9 @@ __device__ __forceinline__ void bulk_s2g(void *gdst, const void *smem_src, unsig
                : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read0() {
-  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+// at most one bulk group (the newest store) may still be reading shared memory
+__device__ __forceinline__ void bulk_wait_read1() {
+  asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
 }
 __device__ __forceinline__ void bulk_wait_all() {
   asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
@@ -358,7 +359,7 @@ __device__ __forceinline__ bool bulk_copy_1t(const BulkRing &ring, char *dst, co
     // had a whole load wait to finish reading, while this one just started
     const unsigned long long n = c - 1 + S;
     if (c >= 1 && n < nch) {
-      asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+      bulk_wait_read1();
       const unsigned ps = (unsigned)((c - 1) % S);
       unsigned nlen = (unsigned)((bytes - n * SB) < SB ? (bytes - n * SB) : SB);
       mbar_expect_tx(ring.mbar + ps, nlen);
