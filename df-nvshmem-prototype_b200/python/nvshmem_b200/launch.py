@@ -25,8 +25,9 @@ def launch(cmd: list[str], npes: int, heap: int | None = None, timeout: float | 
            devices: int | None = None) -> list[int]:
     """Runs `cmd` as `npes` PE processes; returns their exit statuses (a PE
     stopped because another failed -- with stop_on_failure -- or because the
-    timeout passed reports -9).  With `devices`, PE k runs on device
-    k % devices (NVSHMEM_DEVICE)."""
+    timeout passed reports -9).  With `devices`, the PEs are split into
+    contiguous blocks, one per device: PE k runs on device k * devices // npes
+    (NVSHMEM_DEVICE), so neighbouring PEs share a GPU."""
     if npes < 1:
         raise ValueError("npes must be at least 1")
     rdv = tempfile.mkdtemp(prefix="nvshm-")
@@ -38,7 +39,7 @@ def launch(cmd: list[str], npes: int, heap: int | None = None, timeout: float | 
             if heap:
                 e["NVSHMEM_HEAP_SIZE"] = str(heap)
             if devices:
-                e["NVSHMEM_DEVICE"] = str(pe % devices)
+                e["NVSHMEM_DEVICE"] = str(pe * devices // npes)
             procs.append(subprocess.Popen(cmd, env=e, cwd=cwd))
         deadline = None if timeout is None else time.monotonic() + timeout
         codes: list[int | None] = [None] * npes
@@ -71,7 +72,7 @@ def main() -> int:
     ap.add_argument("--heap", type=int, default=None, help="bytes per PE (NVSHMEM_HEAP_SIZE)")
     ap.add_argument("--timeout", type=float, default=None, help="seconds before every PE is stopped")
     ap.add_argument("--devices", type=int, default=None,
-                    help="spread the PEs over this many GPUs (PE k on device k %% devices)")
+                    help="spread the PEs over this many GPUs in contiguous blocks (PE k on device k * D // n)")
     ap.add_argument("cmd", nargs=argparse.REMAINDER)
     a = ap.parse_args()
     cmd = a.cmd[1:] if a.cmd and a.cmd[0] == "--" else a.cmd

@@ -34,4 +34,4 @@ def test_devices_spread_the_pes(tmp_path):
     code = ("import os, sys; open(os.path.join(sys.argv[1], 'pe' + os.environ['NVSHMEM_PROCESS_PE']), 'w')"
             ".write(os.environ.get('NVSHMEM_DEVICE', '-'))")
     assert launch([sys.executable, "-c", code, str(tmp_path)], 5, devices=2) == [0] * 5
-    assert [(tmp_path / f"pe{k}").read_text() for k in range(5)] == ["0", "1", "0", "1", "0"]
+    assert [(tmp_path / f"pe{k}").read_text() for k in range(5)] == ["0", "0", "0", "1", "1"]

@@ -42,8 +42,8 @@ def visible_devices():
 
 @pytest.mark.parametrize("npes,spread", [(2, False), (4, False), (4, True)])
 def test_processes_exchange_blocks(tmp_path, npes, spread):
-    """spread: the launcher's --devices over every visible GPU (PE k on
-    device k % count; on a one-GPU box every PE names device 0)."""
+    """spread: the launcher's --devices over every visible GPU (contiguous
+    blocks of PEs per device; on a one-GPU box every PE names device 0)."""
     exe = build(tmp_path)
     heap = 4 << 20
     codes = launch([exe, "exchange", str(tmp_path)], npes, heap=heap, timeout=240,
