@@ -6,8 +6,8 @@ stand-in for the prototype's ``mpirun -np N ./app`` (no MPI is needed).
 Every process gets NVSHMEM_NPES, NVSHMEM_PROCESS_PE and NVSHMEM_RENDEZVOUS
 (a fresh private directory where the processes exchange their slices' VMM
 handles and share the host barrier); ``nvstart_pes()`` in the application
-picks them up.  The exit status is the first non-zero status of a PE
-process, and when one process fails the others are stopped.
+picks them up.  When one process fails the others are stopped, and the exit
+status is the failed process's status (the first in PE order, if several).
 """
 from __future__ import annotations
 
@@ -79,7 +79,9 @@ def main() -> int:
     if not cmd:
         ap.error("no command")
     codes = launch(cmd, a.npes, a.heap, a.timeout, devices=a.devices)
-    return next((c for c in codes if c != 0), 0)
+    # the PE that failed, not one the launcher stopped because of it (-9)
+    failed = [c for c in codes if c not in (0, -9)]
+    return failed[0] if failed else next((c for c in codes if c != 0), 0)
 
 
 if __name__ == "__main__":

@@ -35,3 +35,25 @@ def test_devices_spread_the_pes(tmp_path):
             ".write(os.environ.get('NVSHMEM_DEVICE', '-'))")
     assert launch([sys.executable, "-c", code, str(tmp_path)], 5, devices=2) == [0] * 5
     assert [(tmp_path / f"pe{k}").read_text() for k in range(5)] == ["0", "0", "0", "1", "1"]
+
+
+def test_command_line_runs_the_pes_and_returns_the_first_failure(tmp_path):
+    """python -m nvshmem_b200.launch -n N [--devices D] -- cmd: every PE runs
+    with its environment, and the exit status is the first non-zero one."""
+    import os
+    import subprocess
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "df-nvshmem-prototype_b200",
+                       "python")
+    env = dict(os.environ, PYTHONPATH=pkg + os.pathsep + os.environ.get("PYTHONPATH", ""))
+    # PE 3 fails once the others have written their files (bounded wait)
+    code = ("import os, sys, time; e = os.environ; pe = int(e['NVSHMEM_PROCESS_PE']); d = sys.argv[1]; "
+            "open(os.path.join(d, 'pe%d' % pe), 'w').write(e['NVSHMEM_DEVICE']); "
+            "t = time.time() + 30\n"
+            "while pe == 3 and time.time() < t and not all(os.path.exists(os.path.join(d, 'pe%d' % k)) for k in range(3)):"
+            " time.sleep(0.01)\n"
+            "sys.exit(7 if pe == 3 else 0)")
+    r = subprocess.run([sys.executable, "-m", "nvshmem_b200.launch", "-n", "4", "--devices", "2", "--timeout", "60",
+                        "--", sys.executable, "-c", code, str(tmp_path)], env=env, capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 7, r.stderr
+    assert [(tmp_path / f"pe{k}").read_text() for k in range(4)] == ["0", "0", "1", "1"]
