@@ -69,14 +69,46 @@ __device__ __forceinline__ bool piece_may_run(BatchCtl *ctl, BatchCtl *sctl) {
 }
 
 // ------------------------------------------------------------------- plan
+// A compact request (nvshmemx_request_compact) in its full form; one that
+// the compact form cannot hold (bits outside its fields, a PUT/GET of 4 GiB
+// or more, P of a double) gets an invalid op, which planning reports.
+__device__ __forceinline__ nvshmemx_request expand_compact(const uint4 q) {
+  nvshmemx_request r;
+  const unsigned op = (q.w >> 20) & 7u, dt = (q.w >> 23) & 3u;
+  r.src_off = (unsigned long long)q.x * 4;
+  r.dst_off = (unsigned long long)q.y * 4;
+  r.bytes = 0;
+  r.src_pe = (uint16_t)(q.w & 1023u);
+  r.dst_pe = (uint16_t)((q.w >> 10) & 1023u);
+  r.op = (uint8_t)op;
+  r.dtype = (uint8_t)dt;
+  r.flags = 0;
+  r.value = 0;
+  bool ok = (q.w >> 25) == 0;
+  if (op == NVSHMEMX_REQ_PUT || op == NVSHMEMX_REQ_GET) {
+    ok = ok && q.z < (1u << 30);
+    r.bytes = q.z * 4u;
+  } else if (op == NVSHMEMX_REQ_SIGNAL) {
+    r.value = (int)q.z;
+  } else if (op == NVSHMEMX_REQ_P) {
+    ok = ok && dt != NVSHMEMX_DT_DOUBLE;
+    r.src_off = q.x;  // the element's bits
+  }
+  if (!ok) r.op = 0xff;
+  return r;
+}
+
 // A batch is planned as one piece, or (pipelined submit) as consecutive
 // pieces planned in order on one stream: piece k appends its items after
 // those of piece k-1 (`prev`) and reports errors, with request indices offset
-// by `req_base`, in its own control block `sctl`.
-__global__ void __launch_bounds__(256) batch_plan_kernel(Cfg c, const nvshmemx_request *__restrict__ reqs, int n,
+// by `req_base`, in its own control block `sctl`.  COMPACT: `reqs_in` holds
+// compact requests, and each is also stored in full form at keep[i].
+template <bool COMPACT>
+__global__ void __launch_bounds__(256) batch_plan_kernel(Cfg c, const void *__restrict__ reqs_in, int n,
                                                          unsigned chunk, WorkItem *__restrict__ items,
                                                          unsigned long long cap, BatchCtl *ctl, BatchCtl *sctl,
-                                                         const BatchCtl *prev, int req_base) {
+                                                         const BatchCtl *prev, int req_base,
+                                                         nvshmemx_request *__restrict__ keep) {
   __shared__ unsigned warp_sums[8];
   __shared__ unsigned long long block_base;
   pdl_release_dependents();
@@ -92,7 +124,17 @@ __global__ void __launch_bounds__(256) batch_plan_kernel(Cfg c, const nvshmemx_r
   w.value = 0;
   w.pad = 0;
   if (i < n) {
-    const nvshmemx_request r = reqs[i];
+    nvshmemx_request r;
+    if (COMPACT) {
+      r = expand_compact(reinterpret_cast<const uint4 *>(reqs_in)[i]);
+      uint4 lo, hi;
+      memcpy(&lo, &r, 16);
+      memcpy(&hi, reinterpret_cast<const char *>(&r) + 16, 16);
+      reinterpret_cast<uint4 *>(keep + i)[0] = lo;
+      reinterpret_cast<uint4 *>(keep + i)[1] = hi;
+    } else {
+      r = reinterpret_cast<const nvshmemx_request *>(reqs_in)[i];
+    }
     const unsigned width = r.dtype == NVSHMEMX_DT_DOUBLE ? 8u : 4u;
     const bool pe_ok = r.src_pe < c.npes && r.dst_pe < c.npes && r.dtype <= NVSHMEMX_DT_DOUBLE;
     const unsigned long long dst = (unsigned long long)c.arena + ((unsigned long long)r.dst_pe << c.log2_stride) + r.dst_off;
@@ -720,6 +762,7 @@ struct nvshmemx_batch {
   int min_chunk = 256;
   unsigned long long cap = 0;
   nvshmemx_request *d_reqs = nullptr;
+  nvshmemx_request_compact *d_reqs_compact = nullptr;  // compact submits: what crossed the host link
   WorkItem *d_items = nullptr;
   BatchCtl *d_ctl = nullptr;
   nvshmemx_request *h_reqs = nullptr;  // pinned
@@ -802,8 +845,10 @@ static int enqueue_stream(nvshmemx_batch *b, bool with_events, const nvshmemx_re
 // Plan (parts & 1) and/or exec (parts & 2) of one piece of a batch (n
 // requests at `src`) on stream `st`, with the piece's control block `ctl`,
 // errors into `sctl`, and its items appended after those of `prev`.
-enum { kPlan = 1, kExec = 2 };
-static int enqueue_piece(nvshmemx_batch *b, bool with_events, const nvshmemx_request *src, int n, BatchCtl *ctl,
+// kCompact: `src` holds compact requests; the plan stores their full form at
+// b->d_reqs + req_base.
+enum { kPlan = 1, kExec = 2, kCompact = 4 };
+static int enqueue_piece(nvshmemx_batch *b, bool with_events, const void *src, int n, BatchCtl *ctl,
                          BatchCtl *sctl, const BatchCtl *prev, int req_base, cudaStream_t st, int parts) {
   const Runtime &r = rt();
   const Cfg c = r.cfg;
@@ -816,9 +861,14 @@ static int enqueue_piece(nvshmemx_batch *b, bool with_events, const nvshmemx_req
                 k.tma_stages);
   (void)cudaGetLastError();  // report only this enqueue's own launch errors
   if (with_events) cudaEventRecord(b->ev_plan0, st);
-  if ((parts & kPlan) && n > 0)
-    batch_plan_kernel<<<(n + 255) / 256, 256, 0, st>>>(c, src, n, (unsigned)k.chunk_bytes, b->d_items, cap_end, ctl,
-                                                       sctl, prev, req_base);
+  if ((parts & kPlan) && n > 0) {
+    if (parts & kCompact)
+      batch_plan_kernel<true><<<(n + 255) / 256, 256, 0, st>>>(c, src, n, (unsigned)k.chunk_bytes, b->d_items, cap_end,
+                                                              ctl, sctl, prev, req_base, b->d_reqs + req_base);
+    else
+      batch_plan_kernel<false><<<(n + 255) / 256, 256, 0, st>>>(c, src, n, (unsigned)k.chunk_bytes, b->d_items,
+                                                               cap_end, ctl, sctl, prev, req_base, nullptr);
+  }
   if (with_events) cudaEventRecord(b->ev_exec0, st);
   if (!(parts & kExec)) return check_cuda(cudaGetLastError(), "batch plan launch");
   const size_t smem = tfn ? tma_smem_bytes(k) : 0;
@@ -924,6 +974,8 @@ int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes
   if (b->cfg.chunk_bytes < min_chunk_bytes) b->cfg.chunk_bytes = (min_chunk_bytes + 255) / 256 * 256;
   int rc = 0;
   if ((rc = check_cuda(cudaMalloc(&b->d_reqs, (size_t)max_requests * sizeof(nvshmemx_request)), "cudaMalloc(reqs)")) ||
+      (rc = check_cuda(cudaMalloc(&b->d_reqs_compact, (size_t)max_requests * sizeof(nvshmemx_request_compact)),
+                       "cudaMalloc(compact reqs)")) ||
       (rc = check_cuda(cudaMalloc(&b->d_items, (size_t)b->cap * sizeof(WorkItem)), "cudaMalloc(items)")) ||
       (rc = check_cuda(cudaMalloc(&b->d_ctl, 128), "cudaMalloc(ctl)")) ||
       (rc = check_cuda(cudaMallocHost(&b->h_reqs, (size_t)max_requests * sizeof(nvshmemx_request)),
@@ -962,6 +1014,7 @@ int nvshmemx_batch_destroy(nvshmemx_batch *b) {
   if (b->copy_stream) cudaStreamSynchronize(b->copy_stream);
   drop_graph(b);
   if (b->d_reqs) cudaFree(b->d_reqs);
+  if (b->d_reqs_compact) cudaFree(b->d_reqs_compact);
   if (b->d_items) cudaFree(b->d_items);
   if (b->d_ctl) cudaFree(b->d_ctl);
   if (b->h_reqs) cudaFreeHost(b->h_reqs);
@@ -1022,6 +1075,63 @@ int nvshmemx_batch_execute(nvshmemx_batch *b, int reps, float *out_ms) {
   return 0;
 }
 
+// The pieces of a submit (graph configuration): see nvshmemx_batch_submit.
+// `host` holds n requests of `elem` bytes (full or compact form, `flag` 0 or
+// kCompact), copied piece by piece to `dev`.
+static int submit_pieces(nvshmemx_batch *b, const void *host, void *dev, size_t elem, int flag, int pieces,
+                         const int ends[3]) {
+  int rc = 0;
+  // The copy stream copies and plans the pieces in order (each plan
+  // appends its items after the previous piece's); the batch's stream
+  // executes piece k once it is planned and piece k-1 has run.  Each piece
+  // has its own control block; the execs report into the first.
+  rc = check_cuda(cudaStreamWaitEvent(b->copy_stream, b->ev_start, 0), "cudaStreamWaitEvent");
+  if (!rc)
+    rc = check_cuda(cudaMemsetAsync(piece_ctl(b, 0), 0, sizeof(BatchCtl), b->copy_stream), "cudaMemsetAsync");
+  if (!rc)  // blocks 1 and 2 are contiguous (bytes 64..127)
+    rc = check_cuda(cudaMemsetAsync(piece_ctl(b, 1), 0, 2 * sizeof(BatchCtl), b->copy_stream), "cudaMemsetAsync");
+  for (int k = 0, at = 0; k < pieces && !rc; at = ends[k++]) {
+    const int m = ends[k] - at;
+    BatchCtl *ck = piece_ctl(b, k);
+    const char *hsrc = static_cast<const char *>(host) + (size_t)at * elem;
+    char *dsrc = static_cast<char *>(dev) + (size_t)at * elem;
+    if ((rc = check_cuda(cudaMemcpyAsync(dsrc, hsrc, (size_t)m * elem, cudaMemcpyHostToDevice, b->copy_stream),
+                         "cudaMemcpyAsync(requests)")) ||
+        (rc = enqueue_piece(b, false, dsrc, m, ck, ck, k ? piece_ctl(b, k - 1) : nullptr, at, b->copy_stream,
+                            kPlan | flag)) ||
+        (rc = check_cuda(cudaEventRecord(b->ev_piece[k], b->copy_stream), "cudaEventRecord")))
+      break;
+  }
+  for (int k = 0, at = 0; k < pieces && !rc; at = ends[k++]) {
+    if ((rc = check_cuda(cudaStreamWaitEvent(b->stream, b->ev_piece[k], 0), "cudaStreamWaitEvent")) ||
+        (rc = enqueue_piece(b, false, nullptr, ends[k] - at, piece_ctl(b, k), piece_ctl(b, 0), nullptr, at,
+                            b->stream, kExec)))
+      break;
+  }
+  if (rc) {
+    cudaStreamSynchronize(b->copy_stream);
+    cudaStreamSynchronize(b->stream);
+    return rc;
+  }
+  BatchCtl *c0 = piece_ctl(b, 0);
+  // the status word reaches the host from a kernel that starts while the
+  // last exec runs and writes as soon as it is done (no copy to schedule)
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(1);
+  lc.blockDim = dim3(32);
+  lc.stream = b->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = attr;
+  lc.numAttrs = 1;
+  if ((rc = check_cuda(cudaLaunchKernelEx(&lc, status_to_host_kernel, (const BatchCtl *)c0,
+                                          (volatile int *)b->h_status_dev),
+                       "status kernel launch")))
+    return rc;
+  return 0;
+}
+
 int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n, int *out_status, float *out_ms) {
   if (!b || n < 0 || n > b->max_n || (n && !reqs)) return fail(NVSHMEMX_ERR_INVALID, "batch_submit: bad arguments");
   int rc;
@@ -1033,53 +1143,7 @@ int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n
   b->timed_direct = false;
   cudaEventRecord(b->ev_start, b->stream);
   if (pieces > 1) {
-    // The copy stream copies and plans the pieces in order (each plan
-    // appends its items after the previous piece's); the batch's stream
-    // executes piece k once it is planned and piece k-1 has run.  Each piece
-    // has its own control block; the execs report into the first.
-    rc = check_cuda(cudaStreamWaitEvent(b->copy_stream, b->ev_start, 0), "cudaStreamWaitEvent");
-    if (!rc)
-      rc = check_cuda(cudaMemsetAsync(piece_ctl(b, 0), 0, sizeof(BatchCtl), b->copy_stream), "cudaMemsetAsync");
-    if (!rc)  // blocks 1 and 2 are contiguous (bytes 64..127)
-      rc = check_cuda(cudaMemsetAsync(piece_ctl(b, 1), 0, 2 * sizeof(BatchCtl), b->copy_stream), "cudaMemsetAsync");
-    for (int k = 0, at = 0; k < pieces && !rc; at = ends[k++]) {
-      const int m = ends[k] - at;
-      BatchCtl *ck = piece_ctl(b, k);
-      if ((rc = check_cuda(cudaMemcpyAsync(b->d_reqs + at, reqs + at, (size_t)m * sizeof(nvshmemx_request),
-                                           cudaMemcpyHostToDevice, b->copy_stream),
-                           "cudaMemcpyAsync(requests)")) ||
-          (rc = enqueue_piece(b, false, b->d_reqs + at, m, ck, ck, k ? piece_ctl(b, k - 1) : nullptr, at,
-                              b->copy_stream, kPlan)) ||
-          (rc = check_cuda(cudaEventRecord(b->ev_piece[k], b->copy_stream), "cudaEventRecord")))
-        break;
-    }
-    for (int k = 0, at = 0; k < pieces && !rc; at = ends[k++]) {
-      if ((rc = check_cuda(cudaStreamWaitEvent(b->stream, b->ev_piece[k], 0), "cudaStreamWaitEvent")) ||
-          (rc = enqueue_piece(b, false, b->d_reqs + at, ends[k] - at, piece_ctl(b, k), piece_ctl(b, 0), nullptr, at,
-                              b->stream, kExec)))
-        break;
-    }
-    if (rc) {
-      cudaStreamSynchronize(b->copy_stream);
-      cudaStreamSynchronize(b->stream);
-      return rc;
-    }
-    BatchCtl *c0 = piece_ctl(b, 0);
-    // the status word reaches the host from a kernel that starts while the
-    // last exec runs and writes as soon as it is done (no copy to schedule)
-    cudaLaunchConfig_t lc = {};
-    lc.gridDim = dim3(1);
-    lc.blockDim = dim3(32);
-    lc.stream = b->stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    lc.attrs = attr;
-    lc.numAttrs = 1;
-    if ((rc = check_cuda(cudaLaunchKernelEx(&lc, status_to_host_kernel, (const BatchCtl *)c0,
-                                            (volatile int *)b->h_status_dev),
-                         "status kernel launch")))
-      return rc;
+    if ((rc = submit_pieces(b, reqs, b->d_reqs, sizeof(nvshmemx_request), 0, pieces, ends))) return rc;
   } else {
     if (n && (rc = check_cuda(cudaMemcpyAsync(b->d_reqs, reqs, (size_t)n * sizeof(nvshmemx_request),
                                               cudaMemcpyHostToDevice, b->stream),
@@ -1092,6 +1156,37 @@ int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n
   }
   cudaEventRecord(b->ev_stop, b->stream);
   if ((rc = check_cuda(cudaStreamSynchronize(b->stream), "batch_submit"))) return rc;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, b->ev_start, b->ev_stop);
+  if (out_ms) *out_ms = ms;
+  if (out_status) *out_status = b->h_status[0];
+  return 0;
+}
+
+int nvshmemx_batch_submit_compact(nvshmemx_batch *b, const nvshmemx_request_compact *reqs, int n, int *out_status,
+                                  float *out_ms) {
+  if (!b || n < 0 || n > b->max_n || (n && !reqs))
+    return fail(NVSHMEMX_ERR_INVALID, "batch_submit_compact: bad arguments");
+  if (b->cfg.stream) return fail(NVSHMEMX_ERR_INVALID, "batch_submit_compact: needs a graph configuration (stream 0)");
+  int rc;
+  b->n = n;
+  b->timed_direct = false;
+  if (out_status) *out_status = 0;
+  if (out_ms) *out_ms = 0.f;
+  if (n == 0) {
+    b->last_pieces = 1;
+    return 0;
+  }
+  // every piece count goes through the copy stream: the plan kernels expand
+  // the compact requests and leave the full form in b->d_reqs
+  int ends[3];
+  const int pieces = split_pieces(n, ends);
+  b->last_pieces = pieces;
+  cudaEventRecord(b->ev_start, b->stream);
+  if ((rc = submit_pieces(b, reqs, b->d_reqs_compact, sizeof(nvshmemx_request_compact), kCompact, pieces, ends)))
+    return rc;
+  cudaEventRecord(b->ev_stop, b->stream);
+  if ((rc = check_cuda(cudaStreamSynchronize(b->stream), "batch_submit_compact"))) return rc;
   float ms = 0;
   cudaEventElapsedTime(&ms, b->ev_start, b->ev_stop);
   if (out_ms) *out_ms = ms;
@@ -1262,8 +1357,8 @@ extern "C" int nvshmemx_batch_execute_noalloc(const nvshmemx_request *d_reqs, in
   // rewritten by the plan kernel before the exec kernel reads it.
   if ((rc = check_cuda(cudaMemsetAsync(ctl, 0, sizeof(BatchCtl), s), "cudaMemsetAsync(noalloc control)"))) return rc;
   if (n > 0)
-    batch_plan_kernel<<<(n + 255) / 256, 256, 0, s>>>(r.cfg, d_reqs, n, (unsigned)k.chunk_bytes, items,
-                                                      kNoallocMaxItems, ctl, ctl, nullptr, 0);
+    batch_plan_kernel<false><<<(n + 255) / 256, 256, 0, s>>>(r.cfg, d_reqs, n, (unsigned)k.chunk_bytes, items,
+                                                             kNoallocMaxItems, ctl, ctl, nullptr, 0, nullptr);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, k.threads, 0);
   if (per_sm < 1) per_sm = 1;

@@ -12,8 +12,8 @@ from ._lib import (CMP_EQ, CMP_GE, CMP_GT, CMP_LE, CMP_LT, CMP_NE, DT_DOUBLE,
                    ERR_INVALID, ERR_NOMEM, ERR_STATE, ERR_TIMEOUT, ERRORS_EXIT,
                    ERRORS_RETURN, LIB_PATH, MODE_BLOCK, MODE_BULK, MODE_THREAD,
                    MODE_WARP, REQ_G, REQ_GET, REQ_P, REQ_PUT, REQ_SIGNAL,
-                   REQUEST_DTYPE, SUCCESS, TRACE_DTYPE, BatchConfig,
+                   REQUEST_COMPACT_DTYPE, REQUEST_DTYPE, SUCCESS, TRACE_DTYPE, BatchConfig,
                    ShmemError)
-from .api import Batch, Shmem, default_batch_config, requests_bytes
+from .api import Batch, Shmem, default_batch_config, requests_bytes, to_compact
 
 __all__ = [n for n in dir() if not n.startswith("__")]

@@ -35,6 +35,11 @@ REQUEST_DTYPE = np.dtype([
 ])
 assert REQUEST_DTYPE.itemsize == 32
 
+# nvshmemx_request_compact: offsets / 4, PUT-GET bytes / 4 or SIGNAL value,
+# meta = src_pe | dst_pe << 10 | op << 20 | dtype << 23
+REQUEST_COMPACT_DTYPE = np.dtype([("src_off4", "<u4"), ("dst_off4", "<u4"), ("arg", "<u4"), ("meta", "<u4")])
+assert REQUEST_COMPACT_DTYPE.itemsize == 16
+
 TRACE_DTYPE = np.dtype([
     ("t_ns", "<i8"), ("spin_ns", "<i8"), ("local_addr", "<u8"), ("remote_addr", "<u8"),
     ("bytes", "<u4"), ("op", "<u2"), ("pe", "<u2"), ("peer", "<u2"), ("tid", "<u2"),
@@ -133,6 +138,7 @@ _SIGS = {
     "nvshmemx_batch_execute": (c_int, [c_void_p, c_int, _P(c_float)]),
     "nvshmemx_batch_execute_direct": (c_int, [c_void_p, c_int, _P(c_float), _P(c_float)]),
     "nvshmemx_batch_submit": (c_int, [c_void_p, c_void_p, c_int, _P(c_int), _P(c_float)]),
+    "nvshmemx_batch_submit_compact": (c_int, [c_void_p, c_void_p, c_int, _P(c_int), _P(c_float)]),
     "nvshmemx_batch_last_stats": (c_int, [c_void_p, _P(c_ulonglong), _P(c_float), _P(c_float)]),
     "nvshmemx_requests_bytes": (c_ulonglong, [c_void_p, c_int]),
     "nvshmemx_batch_execute_percall": (c_int, [c_void_p, c_int, c_int, _P(c_float)]),

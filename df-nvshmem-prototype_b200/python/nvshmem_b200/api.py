@@ -243,6 +243,21 @@ class Batch:
         self.n = n
         return st.value, ms.value
 
+    def submit_compact(self, reqs: np.ndarray, n: int | None = None):
+        """submit() for requests in the 16-byte compact form (to_compact)."""
+        n = len(reqs) if n is None else n
+        st = c_int(0)
+        ms = c_float(0)
+        check(lib.nvshmemx_batch_submit_compact(self.h, ptr(reqs), n, byref(st), byref(ms)), "batch_submit_compact")
+        self.n = n
+        return st.value, ms.value
+
+    def host_buffer_compact(self) -> np.ndarray:
+        """The batch's pinned request buffer viewed as compact requests."""
+        p = lib.nvshmemx_batch_host_buffer(self.h)
+        raw = (ctypes.c_char * (self.max_requests * 32)).from_address(p)
+        return np.frombuffer(raw, dtype=L.REQUEST_COMPACT_DTYPE)
+
     def percall(self, mode: int = L.MODE_THREAD, reps: int = 1) -> float:
         ms = c_float(0)
         check(lib.nvshmemx_batch_execute_percall(self.h, mode, reps, byref(ms)), "batch_percall")
@@ -254,6 +269,31 @@ class Batch:
         e = c_float(0)
         check(lib.nvshmemx_batch_last_stats(self.h, byref(ch), byref(p), byref(e)), "batch_stats")
         return ch.value, p.value, e.value
+
+
+def to_compact(reqs: np.ndarray) -> np.ndarray:
+    """The 16-byte compact form of full requests (nvshmemx_request_compact);
+    ValueError for a request it cannot hold (offsets or PUT/GET sizes not
+    multiples of 4 or too large, PEs of 1024 and more, P of a double)."""
+    r = np.ascontiguousarray(reqs, dtype=L.REQUEST_DTYPE)
+    op, dt = r["op"].astype(np.uint32), r["dtype"].astype(np.uint32)
+    is_p = op == L.REQ_P
+    is_copy = (op == L.REQ_PUT) | (op == L.REQ_GET)
+    off_src = np.where(is_p, 0, r["src_off"])
+    bad = ((off_src % 4 != 0) | (r["dst_off"] % 4 != 0) | (off_src >= (16 << 30)) | (r["dst_off"] >= (16 << 30))
+           | (r["src_pe"] >= 1024) | (r["dst_pe"] >= 1024) | (op > 7) | (dt > 3)
+           | (is_copy & (r["bytes"] % 4 != 0)) | (is_p & ((dt == L.DT_DOUBLE) | (r["src_off"] >= (1 << 32)))))
+    if bad.any():
+        raise ValueError(f"request {int(np.flatnonzero(bad)[0])} has no compact form")
+    out = np.zeros(len(r), dtype=L.REQUEST_COMPACT_DTYPE)
+    out["src_off4"] = np.where(is_p, r["src_off"], r["src_off"] // 4).astype(np.uint32)
+    out["dst_off4"] = (r["dst_off"] // 4).astype(np.uint32)
+    arg = np.zeros(len(r), dtype=np.uint32)
+    arg = np.where(is_copy, r["bytes"] // 4, arg)
+    arg = np.where(op == L.REQ_SIGNAL, r["value"].astype(np.int64) & 0xFFFFFFFF, arg)
+    out["arg"] = arg.astype(np.uint32)
+    out["meta"] = (r["src_pe"].astype(np.uint32) | (r["dst_pe"].astype(np.uint32) << 10) | (op << 20) | (dt << 23))
+    return out
 
 
 def requests_bytes(reqs: np.ndarray) -> int:

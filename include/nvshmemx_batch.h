@@ -99,6 +99,17 @@ int nvshmemx_batch_execute(nvshmemx_batch *b, int reps, float *out_ms);
 int nvshmemx_batch_submit(nvshmemx_batch *b, const nvshmemx_request *reqs, int n, int *out_status,
                           float *out_ms);
 
+/* nvshmemx_batch_submit for requests in the 16-byte compact form
+ * (nvshmemx_ops.h), which halves the host-to-device copy; the batch's host
+ * buffer, viewed as nvshmemx_request_compact, is the pinned place for them.
+ * Same pieces, order and error rules as nvshmemx_batch_submit; the plan
+ * kernels expand each request as they read it and leave the full 32-byte
+ * form resident, so nvshmemx_batch_execute afterwards runs the same batch.
+ * A compact request with bits set outside its fields is reported as
+ * NVSHMEMX_ERR_INVALID.  Needs a graph configuration (stream 0). */
+int nvshmemx_batch_submit_compact(nvshmemx_batch *b, const nvshmemx_request_compact *reqs, int n,
+                                  int *out_status, float *out_ms);
+
 /* The same work as nvshmemx_batch_execute, enqueued without a graph and with
  * CUDA events around the plan and exec kernels on the batch's stream:
  * *out_ms is the time of all reps, *out_exec_ms the exec kernel's share. */

@@ -52,6 +52,21 @@ typedef struct nvshmemx_request {
   int32_t value;     /* SIGNAL value                                         */
 } nvshmemx_request;
 
+/* Compact form of a request (16 bytes) for nvshmemx_batch_submit_compact,
+ * which halves what crosses the host link.  It holds every request whose
+ * offsets and sizes are multiples of 4 below 16 GiB and whose PEs are below
+ * 1024, except P of a double (64-bit value):
+ *   src_off4  src_off / 4 (P: the int or float element's bits)
+ *   dst_off4  dst_off / 4
+ *   arg       PUT / GET: bytes / 4; SIGNAL: value; P, G: 0
+ *   meta      src_pe | dst_pe << 10 | op << 20 | dtype << 23 (bits 25-31 0) */
+typedef struct nvshmemx_request_compact {
+  uint32_t src_off4;
+  uint32_t dst_off4;
+  uint32_t arg;
+  uint32_t meta;
+} nvshmemx_request_compact;
+
 /* How a request is carried out (the per-call variants). */
 #define NVSHMEMX_MODE_THREAD 0 /* one thread per request, nvshmem_{T}_put/get/p/g */
 #define NVSHMEMX_MODE_WARP 1   /* one warp per request, nvshmemx_{T}_put/get_warp  */

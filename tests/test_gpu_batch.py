@@ -170,6 +170,58 @@ def test_submit_pipelined(shmem_factory, cfg, n):
     sh.status()
 
 
+@pytest.mark.parametrize("n", [5000, 20000], ids=["one_piece", "two_pieces"])
+@pytest.mark.parametrize("cfg", [None, CONFIGS[0]], ids=["tma", "register"])
+def test_submit_compact(shmem_factory, cfg, n):
+    """The 16-byte compact form through the pinned buffer: the same heaps as
+    the oracle, the full form left resident for later executions, and an
+    invalid compact request in the last piece reported after the pieces
+    before it have run."""
+    from nvshmem_b200 import ERR_INVALID, to_compact
+    npes, heap = 16, 32 << 20
+    reqs = c4_batch(seed=49, n=n, npes=npes, heap=heap, hi=16 << 10)
+    sh, om = setup(shmem_factory, npes, heap)
+    with sh.batch(len(reqs), int(reqs["bytes"].sum()), 256) as b:
+        if cfg:
+            b.set_config(cfg)
+        buf = b.host_buffer_compact()
+        buf[:n] = to_compact(reqs)
+        st, ms = b.submit_compact(buf, n)
+        assert st == 0 and ms > 0
+        om.apply_requests(reqs)
+        assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+        b.execute(1)  # runs the expanded requests the plan kernels left
+        assert sh.status() == 0
+        assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+        # bits outside the fields of one request of the last piece
+        last = split_ends(n)
+        n0 = last[-2] if len(last) > 1 else 0
+        for pe in range(npes):
+            sh.fill_random(pe, 0, heap, 8)
+        om2 = Model(npes, heap)
+        for pe in range(npes):
+            om2.fill_random(pe, 0, heap, 8)
+        bad = to_compact(reqs)
+        bad[n0 + 7]["meta"] |= 1 << 30
+        buf[:n] = bad
+        st, _ = b.submit_compact(buf, n)
+        assert st == ERR_INVALID
+        om2.apply_requests(reqs[:n0])
+        assert first_diff(heap_images(sh, npes, heap), om2.heap) is None
+    sh.status()
+
+
+def test_submit_compact_needs_a_graph_configuration(shmem_factory):
+    from nvshmem_b200 import ShmemError, to_compact
+    sh, _ = setup(shmem_factory, 4, 1 << 20)
+    reqs = c4_batch(seed=50, n=100, npes=4, heap=1 << 20, hi=1024)
+    with sh.batch(len(reqs), int(reqs["bytes"].sum()), 256) as b:
+        b.set_config(STREAM)
+        with pytest.raises(ShmemError):
+            b.submit_compact(to_compact(reqs))
+    sh.status()
+
+
 def test_stream_submit(shmem_factory):
     """End-to-end in stream mode (copy, then the streaming kernel): batches of
     several sizes in a row through the pinned buffer and from ordinary
