@@ -38,6 +38,14 @@ WORKLOAD = ("C4 batched uneven traffic: 64 virtual PEs x 64 MiB heap, 100,000 pu
             "requests per batch, log-normal sizes median 2 KiB sigma 1.5 clipped 4 B..4 MiB, "
             "put 45%/get 45%/signal 10%, uniform PE pairs, disjoint 16-B-aligned destinations, seed 4")
 TUNED = os.path.join(ROOT, "df-nvshmem-prototype_b200", "tuned", "batch_c4.json")
+
+
+def line_config(alg, world):
+    """The `config` object of both arms' JSON lines (identical by design)."""
+    return {"workload": WORKLOAD,
+            "l2": "inputs larger than L2 (64 x 64 MiB heap); the GPU arm also flushes L2 between steps "
+                  "(256 MiB write)",
+            "alg_bytes_per_step": int(alg), "parallelism": f"replicas x{world}"}
 NCU_SUMMARY = os.path.join(ROOT, "profiles", "batch_exec_c4.json")
 
 
@@ -125,7 +133,9 @@ def barrier(dist):
 
 
 # ------------------------------------------------------------ CPU baseline
-def cpu_baseline(reqs, npes, heap, max_seconds=12.0, warmup=1):
+def cpu_baseline(reqs, npes, heap, max_seconds=12.0, warmup=1, reps=1000000):
+    """The host path timed on this machine's cores: `reps` executions of the
+    batch (at most `max_seconds` of them) by npes forked ranks."""
     from oracle import model as om  # the checker package; only this leg runs it
     if not os.path.exists(om.HOST_BENCH):
         om.build()
@@ -133,7 +143,7 @@ def cpu_baseline(reqs, npes, heap, max_seconds=12.0, warmup=1):
         f.write(reqs.tobytes())
         path = f.name
     try:
-        out = subprocess.run([om.HOST_BENCH, "batch", path, str(npes), str(heap), "1000000", str(max_seconds), "44",
+        out = subprocess.run([om.HOST_BENCH, "batch", path, str(npes), str(heap), str(reps), str(max_seconds), "44",
                               str(warmup)],
                              capture_output=True, text=True, timeout=600, check=True).stdout
     finally:
@@ -142,7 +152,7 @@ def cpu_baseline(reqs, npes, heap, max_seconds=12.0, warmup=1):
     return {"value": round(r["gbs"], 3), "unit": UNIT, "cores": r["cores"], "kind": "port",
             "ms_per_step": 1e3 * r["seconds_per_rep"], "reps": r["reps"],
             "sample": f"the full {r['requests']}-request batch, {r['npes']} forked ranks, {r['reps']} reps "
-                      f"within {max_seconds:.0f} s (host has {r['host_cores']} cores)",
+                      f"in {r['reps'] * r['seconds_per_rep']:.1f} s (host has {r['host_cores']} cores)",
             "heap_checksum": r["heap_checksum"]}
 
 
@@ -151,15 +161,23 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     import numpy as np  # noqa: F401
+    from nvshmem_b200._abi import REQ_GET, REQ_PUT, REQ_SIGNAL  # constants only: the GPU library is not loaded
     from nvshmem_b200.traffic import c4_batch
     reqs = c4_batch(**C4)
+    copies = (reqs["op"] == REQ_PUT) | (reqs["op"] == REQ_GET)
+    alg = 2 * int(reqs["bytes"][copies].astype(np.int64).sum()) + 4 * int((reqs["op"] == REQ_SIGNAL).sum())
     t0 = time.time()
-    cb = cpu_baseline(reqs, C4["npes"], C4["heap"], max_seconds=max(5.0, 2.0 * args.steps), warmup=args.warmup)
+    # exactly the requested steps, each one execution of the whole batch by
+    # 64 forked ranks (about 8 ms each); 600 s is only a safety bound
+    cb = cpu_baseline(reqs, C4["npes"], C4["heap"], max_seconds=600.0, warmup=args.warmup, reps=args.steps)
+    assert cb["reps"] == args.steps, cb
     line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": cb["reps"],
             "warmup": args.warmup, "ms_per_step": round(cb["ms_per_step"], 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
             "data": "synthetic (seeded)", "impl": "reference",
-            "config": {"workload": WORKLOAD, "parallelism": "one OS process per PE"},
+            "config": line_config(alg, args.gpus),
+            "parallelism_detail": "one OS process per PE (64 forked ranks), memcpy into a shared mapping, "
+                                  "process-shared pthread barrier",
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": round(time.time() - t0, 1)}
@@ -297,34 +315,77 @@ def run_c2_sweep(peak, only_size=0):
     return out
 
 
+def c3_nbr(pe, d, px=2, py=2, pz=2):
+    """Neighbour of `pe` in direction d (0..5 = -x,+x,-y,+y,-z,+z) on the
+    periodic px x py x pz grid (PE = x + px*(y + py*z))."""
+    x, y, z = pe % px, (pe // px) % py, pe // (px * py)
+    s = 1 if d & 1 else -1
+    if d < 2:
+        x = (x + s) % px
+    elif d < 4:
+        y = (y + s) % py
+    else:
+        z = (z + s) % pz
+    return x + px * (y + py * z)
+
+
+def c3_faces(block, n):
+    """The six faces of one (z, y, x) block as the halo sends them: face d
+    row j is z=j over y (x faces), z=j over x (y faces), y=j over x (z faces)."""
+    b = block.reshape(n, n, n)
+    return [b[:, :, 0], b[:, :, n - 1], b[:, 0, :], b[:, n - 1, :], b[0, :, :], b[n - 1, :, :]]
+
+
 def run_c3_halo(peak, iters=100):
-    """C3: 8 PEs on a periodic 2x2x2 grid, 256^3 float64 per PE, 100
-    iterations of 6 face puts (x faces gathered with stride 256) + int_p
-    signals + int_wait + a barrier: the device barrier inside one persistent
-    launch (headline), and one launch per iteration followed by
-    nvshmem_barrier_all_offload (the prototype's structure)."""
+    """C3: 8 PEs on a periodic 2x2x2 grid, 256^3 float64 per PE (N(0,1),
+    seed 3), 100 iterations of 6 face puts (x faces gathered with stride 256)
+    + int_p signals + int_wait + a barrier: the device barrier inside one
+    persistent launch (headline), and one launch per iteration followed by
+    nvshmem_barrier_all_offload (the prototype's structure).  After each
+    timed run every PE's six ghost faces and six signal words are read back
+    and checked bit for bit against the faces of its neighbours' blocks."""
+    import numpy as np
     from nvshmem_b200 import Shmem
+    from nvshmem_b200.traffic import c3_block
     n = 256
     block, ghosts = n ** 3 * 8, 6 * n * n * 8
     heap = block + ghosts + 4096
+    sig = block + ghosts
+    faces = []
     with Shmem(8, heap) as sh:
         for pe in range(8):
-            sh.fill_random(pe, 0, block, 3)
+            b = c3_block(n, pe)
+            sh.write(pe, 0, b)
+            faces.append([np.ascontiguousarray(f).view(np.uint8).reshape(-1) for f in c3_faces(b, n)])
+            del b
             sh.memset(pe, block, 0, ghosts + 4096)
+
+        def check(tag):
+            for q in range(8):
+                got = sh.read(q, block, ghosts + 24)
+                for g in range(6):
+                    want = faces[c3_nbr(q, g)][g ^ 1]
+                    assert np.array_equal(got[g * n * n * 8:(g + 1) * n * n * 8], want), (tag, q, g)
+                assert np.array_equal(got[ghosts:].view(np.int32), np.full(6, iters, np.int32)), (tag, q)
+
         # ctas_per_pe 0: as many CTAs per PE as stay co-resident (the
         # exchange is latency-bound, so more warps in flight help)
-        sh.halo(2, 2, 2, n, 0, block, block + ghosts, 3, 0)
+        sh.halo(2, 2, 2, n, 0, block, sig, 3, 0)
         for pe in range(8):
-            sh.memset(pe, block + ghosts, 0, 64)
-        ms = sh.halo(2, 2, 2, n, 0, block, block + ghosts, iters, 0)
-        for pe in range(8):
-            sh.memset(pe, block + ghosts, 0, 64)
-        ms_off = sh.halo(2, 2, 2, n, 0, block, block + ghosts, iters, 0, offload=True)
+            sh.memset(pe, block, 0, ghosts + 64)
+        ms = sh.halo(2, 2, 2, n, 0, block, sig, iters, 0)
         assert sh.status() == 0
+        check("persistent")
+        for pe in range(8):
+            sh.memset(pe, block, 0, ghosts + 64)
+        ms_off = sh.halo(2, 2, 2, n, 0, block, sig, iters, 0, offload=True)
+        assert sh.status() == 0
+        check("offload")
     face_bytes = 8 * 6 * n * n * 8
     return {"us_per_iter": round(1e3 * ms / iters, 2), "face_GBps": round(2 * face_bytes * iters / (ms / 1e3) / 1e9, 1),
             "iters": iters, "n": n, "ctas_per_pe": "as many as stay co-resident",
-            "offload_barrier_us_per_iter": round(1e3 * ms_off / iters, 2)}
+            "offload_barrier_us_per_iter": round(1e3 * ms_off / iters, 2),
+            "bit_exact": "every ghost face and signal word of all 8 PEs after each timed run"}
 
 
 def run_c5_picker():
@@ -426,14 +487,17 @@ def run_gpu(args, rank, world, local):
                     flush()
                     b.submit_compact(hc, len(reqs))
                 barrier(dist)
-                e2e_ms = []
+                e2e_ms, e2e_wall = [], []
                 for _ in range(args.steps):
                     flush()
+                    w0 = time.perf_counter()
                     st, ms = b.submit_compact(hc, len(reqs))
+                    e2e_wall.append(time.perf_counter() - w0)
                     assert st == 0, f"batch status {st}"
                     e2e_ms.append(ms)
                 barrier(dist)
                 t_e2e = reduce_max(dist, sum(e2e_ms) / 1e3)
+                t_e2e_wall = reduce_max(dist, sum(e2e_wall))
                 cfg_used = b.config()
             assert sh.status() == 0
             checks = [sh.checksum(pe, 0, C4["heap"]) for pe in range(C4["npes"])]
@@ -448,6 +512,7 @@ def run_gpu(args, rank, world, local):
     value = world * alg * args.steps / t_batch / 1e9
     e2e = world * alg * args.steps / t_e2e / 1e9
     e2e_full = world * alg * args.steps / t_e2e_full / 1e9
+    e2e_wall = world * alg * args.steps / t_e2e_wall / 1e9
     exec_avg = statistics.mean(exec_ms) / 1e3
     achieved = alg / exec_avg / 1e9
     traffic = None
@@ -458,9 +523,8 @@ def run_gpu(args, rank, world, local):
         "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(1e3 * t_batch / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "l2": "flushed between steps (256 MiB write)",
-                   "parallelism": f"replicas x{world}", "batch_config": cfg_used,
-                   "alg_bytes_per_step": alg, "chunks": chunks},
+        "config": line_config(alg, world),
+        "batch_detail": {"batch_config": cfg_used, "chunks": chunks},
         "frac_of_hbm": round(value / peak, 3),
         "percall_GBps": {k: round(v, 2) for k, v in pc.items()},
         "speedup_vs_percall_thread": round(value / pc["thread"], 2),
@@ -468,6 +532,11 @@ def run_gpu(args, rank, world, local):
                 "d2h_bytes_per_step": 8,
                 "mode": ("nvshmemx_batch_submit_compact (16-byte requests from pinned host memory), pipelined: "
                          "the first quarter of the requests executes while the rest is copied"),
+                "timing": ("CUDA events on the batch stream, from before the request copy to after the "
+                           "status word reached host memory"),
+                "host_wall": {"value": round(e2e_wall, 2),
+                              "timing": "host clock around the Python call (ctypes entry to return, the final "
+                                        "stream synchronisation included)"},
                 "full_form": {"value": round(e2e_full, 2), "h2d_bytes_per_step": int(len(reqs) * 32),
                               "call": "nvshmemx_batch_submit (32-byte requests)"}},
         # plan + exec per device-resident step; 2 x (plan + exec) + the

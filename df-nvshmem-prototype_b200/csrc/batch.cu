@@ -69,6 +69,14 @@ __device__ __forceinline__ bool piece_may_run(BatchCtl *ctl, BatchCtl *sctl) {
 }
 
 // ------------------------------------------------------------------- plan
+// [off, off + bytes) lies inside the mapped part of a slice.  Written so that
+// no sum can wrap: off and bytes are caller-supplied 64-bit values, and
+// off + bytes may overflow (off = 2^64 - 4, bytes = 8 would pass a test of
+// the sum and address memory below the slice).
+__device__ __forceinline__ bool range_in_slice(const Cfg &c, unsigned long long off, unsigned long long bytes) {
+  return off <= c.slice_bytes && bytes <= c.slice_bytes - off;
+}
+
 // A compact request (nvshmemx_request_compact) in its full form; one that
 // the compact form cannot hold (bits outside its fields, a PUT/GET of 4 GiB
 // or more, P of a double) gets an invalid op, which planning reports.
@@ -144,7 +152,7 @@ __global__ void __launch_bounds__(256) batch_plan_kernel(Cfg c, const void *__re
       case NVSHMEMX_REQ_GET:
       case NVSHMEMX_REQ_G: {
         const unsigned long long bytes = r.op == NVSHMEMX_REQ_G ? width : r.bytes;
-        if (!pe_ok || r.src_off + bytes > c.slice_bytes || r.dst_off + bytes > c.slice_bytes) {
+        if (!pe_ok || !range_in_slice(c, r.src_off, bytes) || !range_in_slice(c, r.dst_off, bytes)) {
           set_status(sctl, NVSHMEMX_ERR_BOUNDS, req_base + i);
           break;
         }
@@ -157,7 +165,7 @@ __global__ void __launch_bounds__(256) batch_plan_kernel(Cfg c, const void *__re
       case NVSHMEMX_REQ_SIGNAL:
       case NVSHMEMX_REQ_P: {
         const unsigned bytes = r.op == NVSHMEMX_REQ_SIGNAL ? 4u : width;
-        if (!pe_ok || r.dst_off + bytes > c.slice_bytes || (r.dst_off & (bytes - 1))) {
+        if (!pe_ok || !range_in_slice(c, r.dst_off, bytes) || (r.dst_off & (bytes - 1))) {
           set_status(sctl, NVSHMEMX_ERR_BOUNDS, req_base + i);
           break;
         }
@@ -455,7 +463,7 @@ __device__ __forceinline__ void plan_one(const Cfg &c, const nvshmemx_request &r
     case NVSHMEMX_REQ_GET:
     case NVSHMEMX_REQ_G: {
       const unsigned long long bytes = r.op == NVSHMEMX_REQ_G ? width : r.bytes;
-      if (!pe_ok || r.src_off + bytes > c.slice_bytes || r.dst_off + bytes > c.slice_bytes) {
+      if (!pe_ok || !range_in_slice(c, r.src_off, bytes) || !range_in_slice(c, r.dst_off, bytes)) {
         set_status(ctl, NVSHMEMX_ERR_BOUNDS, i);
         return;
       }
@@ -468,7 +476,7 @@ __device__ __forceinline__ void plan_one(const Cfg &c, const nvshmemx_request &r
     case NVSHMEMX_REQ_SIGNAL:
     case NVSHMEMX_REQ_P: {
       const unsigned bytes = r.op == NVSHMEMX_REQ_SIGNAL ? 4u : width;
-      if (!pe_ok || r.dst_off + bytes > c.slice_bytes || (r.dst_off & (bytes - 1))) {
+      if (!pe_ok || !range_in_slice(c, r.dst_off, bytes) || (r.dst_off & (bytes - 1))) {
         set_status(ctl, NVSHMEMX_ERR_BOUNDS, i);
         return;
       }
@@ -1342,8 +1350,14 @@ extern "C" int nvshmemx_batch_execute_noalloc(const nvshmemx_request *d_reqs, in
   } else {
     nvshmemx_batch_default_config(&k);
   }
+  // Streaming mode keeps a launch generation and per-item tags that must
+  // outlive a call; the shared scratch cannot hold them for every caller.
+  if (k.stream != 0)
+    return fail(NVSHMEMX_ERR_INVALID, "batch_execute_noalloc: stream mode is not available here (set stream = 0)");
   ExecFn fn = pick_exec(k.vec_bytes, k.unroll);
-  if (!fn) return fail(NVSHMEMX_ERR_INVALID, "batch_execute_noalloc: no kernel for this configuration");
+  TmaFn tfn = k.tma_stages ? pick_tma(k.tma_stages) : nullptr;
+  if (!fn || (k.tma_stages && !tfn))
+    return fail(NVSHMEMX_ERR_INVALID, "batch_execute_noalloc: no kernel for this configuration");
   void *scratch = nullptr;
   int rc;
   if ((rc = noalloc_scratch(&scratch))) return rc;
@@ -1359,11 +1373,24 @@ extern "C" int nvshmemx_batch_execute_noalloc(const nvshmemx_request *d_reqs, in
   if (n > 0)
     batch_plan_kernel<false><<<(n + 255) / 256, 256, 0, s>>>(r.cfg, d_reqs, n, (unsigned)k.chunk_bytes, items,
                                                              kNoallocMaxItems, ctl, ctl, nullptr, 0, nullptr);
+  // The exec kernel the configuration names: TMA rings (their stages are
+  // shared memory, not scratch) or the register copy.
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, k.threads, 0);
+  const size_t smem = tfn ? tma_smem_bytes(k) : 0;
+  if (tfn) {
+    cudaFuncSetAttribute((const void *)tfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)tfn, k.threads, smem);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, k.threads, 0);
+  }
   if (per_sm < 1) per_sm = 1;
   const int ctas = k.ctas_per_sm > 0 && k.ctas_per_sm < per_sm ? k.ctas_per_sm : per_sm;
-  fn<<<r.sm_count * ctas, k.threads, 0, s>>>(items, ctl, ctl, kNoallocMaxItems, k.grab);
+  if (tfn)
+    tfn<<<r.sm_count * ctas, k.threads, smem, s>>>(items, ctl, ctl, kNoallocMaxItems, k.grab,
+                                                    (unsigned)k.tma_stage_bytes, (unsigned)k.tma_min_bytes,
+                                                    (long long)r.cfg.wait_timeout_ns);
+  else
+    fn<<<r.sm_count * ctas, k.threads, 0, s>>>(items, ctl, ctl, kNoallocMaxItems, k.grab);
   if ((rc = check_cuda(cudaGetLastError(), "batch_execute_noalloc launch"))) return rc;
   int st[2] = {0, 0};
   if ((rc = check_cuda(cudaMemcpyAsync(st, &ctl->status, sizeof st, cudaMemcpyDeviceToHost, s),

@@ -459,6 +459,17 @@ static int last_launch(const char *what) {
   return check_cuda(cudaGetLastError(), what);
 }
 
+// [off, off + bytes) lies inside [0, limit).  Arguments come from the caller
+// as size_t, so the test never forms a sum that could wrap.
+static bool range_ok(size_t off, size_t bytes, size_t limit) { return off <= limit && bytes <= limit - off; }
+
+// *out = a * b, false when the product does not fit a size_t.
+static bool mul_ok(size_t a, size_t b, size_t *out) {
+  if (a != 0 && b > (size_t)-1 / a) return false;
+  *out = a * b;
+  return true;
+}
+
 // Shared memory for the CTA-wide TMA copies: a 64 KiB ring (six stages)
 // plus 128 bytes of mbarriers (three CTAs fit an SM).
 static const unsigned kBulkSmem = 4 * 16384 + 128;
@@ -568,8 +579,8 @@ int nvshmemx_op_pingpong(size_t flag_off, size_t data_off, int len_elems, int it
   if ((rc = need_collective())) return rc;
   const Runtime &r = rt();
   if (r.npes < 2) return fail(NVSHMEMX_ERR_INVALID, "pingpong needs at least 2 PEs");
-  if (iters < 1 || skip < 0 || len_elems < 0 || flag_off + 4 > r.heap_bytes ||
-      data_off + (size_t)len_elems * 4 > r.heap_bytes)
+  if (iters < 1 || skip < 0 || len_elems < 0 || !range_ok(flag_off, 4, r.heap_bytes) ||
+      !range_ok(data_off, (size_t)len_elems * 4, r.heap_bytes))
     return fail(NVSHMEMX_ERR_INVALID, "pingpong: bad arguments");
   long long *cyc = (long long *)g_out_buf.get((size_t)iters * 8 + 64);
   if (!cyc) return fail(NVSHMEMX_ERR_NOMEM, "pingpong scratch");
@@ -657,9 +668,12 @@ static int alltoall_setup(int op, int dtype, size_t send_off, size_t recv_off, s
   if (bytes % w) return fail(NVSHMEMX_ERR_INVALID, "alltoall: bytes not a multiple of the element width");
   if (mode == NVSHMEMX_MODE_THREAD && bytes / w > 0x7fffffffull)
     return fail(NVSHMEMX_ERR_INVALID, "alltoall: message too long for an int element count");
-  const size_t span = (size_t)r.npes * bytes;
-  const size_t last = (size_t)(nsets - 1) * set_stride;
-  if (send_off + last + span > r.heap_bytes || recv_off + last + span > r.heap_bytes)
+  // every set of send and receive buffers, [off + s * set_stride, + npes * bytes)
+  // for s < nsets, must lie inside the heap; no product or sum may wrap
+  size_t span = 0, last = 0;
+  if (!mul_ok((size_t)r.npes, bytes, &span) || !mul_ok((size_t)(nsets - 1), set_stride, &last) ||
+      !range_ok(last, span, r.heap_bytes) || !range_ok(send_off, last + span, r.heap_bytes) ||
+      !range_ok(recv_off, last + span, r.heap_bytes))
     return fail(NVSHMEMX_ERR_INVALID, "alltoall: buffers exceed the heap");
   *smem = mode == NVSHMEMX_MODE_BULK ? kBulkSmem : 0;
   *grid = dim3(ctas_per_pe);
@@ -738,8 +752,10 @@ static int halo_check(int px, int py, int pz, int n, size_t block_off, size_t gh
   if (px < 1 || py < 1 || pz < 1 || px * py * pz != r.npes || n < 1 || iters < 1 || *ctas_per_pe < 1)
     return fail(NVSHMEMX_ERR_INVALID, "halo: grid %dx%dx%d does not match %d PEs", px, py, pz, r.npes);
   const size_t nn = (size_t)n;
-  if (block_off + nn * nn * nn * 8 > r.heap_bytes || ghost_off + 6 * nn * nn * 8 > r.heap_bytes ||
-      sig_off + 24 > r.heap_bytes || (block_off | ghost_off) % 16 || sig_off % 4)
+  size_t face = 0, block = 0, ghosts = 0;
+  if (!mul_ok(nn * 8, nn, &face) || !mul_ok(face, nn, &block) || !mul_ok(face, 6, &ghosts) ||
+      !range_ok(block_off, block, r.heap_bytes) || !range_ok(ghost_off, ghosts, r.heap_bytes) ||
+      !range_ok(sig_off, 24, r.heap_bytes) || (block_off | ghost_off) % 16 || sig_off % 4)
     return fail(NVSHMEMX_ERR_INVALID, "halo: buffers exceed the heap or are misaligned");
   return 0;
 }
@@ -786,7 +802,8 @@ int nvshmemx_op_wait_test(size_t flag_off, int value, long long timeout_ns, int 
   int rc;
   if ((rc = need_collective())) return rc;
   const Runtime &r = rt();
-  if (flag_off + 4 > r.heap_bytes || flag_off % 4) return fail(NVSHMEMX_ERR_INVALID, "wait_test: bad flag offset");
+  if (!range_ok(flag_off, 4, r.heap_bytes) || flag_off % 4)
+    return fail(NVSHMEMX_ERR_INVALID, "wait_test: bad flag offset");
   int *d = (int *)g_out_buf.get(64);
   if (!d) return fail(NVSHMEMX_ERR_NOMEM, "wait_test scratch");
   cudaMemset(d, 0, 4);

@@ -528,7 +528,7 @@ void *nvshmalloc(size_t size) {
   }
   if (t_spmd) {
     size_t off = r.tail[t_pe];
-    if (off + size > r.heap_bytes) {
+    if (size > r.heap_bytes - off) {  // off <= heap_bytes; no sum that could wrap
       fail(NVSHMEMX_ERR_NOMEM,
            "Not enough memory on the heap (set to %zu, can be increased by setting NVSHMEM_HEAP_SIZE)",
            r.heap_bytes);
@@ -546,7 +546,7 @@ void *nvshmalloc(size_t size) {
       return nullptr;
     }
   }
-  if (off + size > r.heap_bytes) {
+  if (size > r.heap_bytes - off) {
     fail(NVSHMEMX_ERR_NOMEM,
          "Not enough memory on the heap (set to %zu, can be increased by setting NVSHMEM_HEAP_SIZE)",
          r.heap_bytes);

@@ -15,7 +15,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from ._lib import (DT_DOUBLE, DT_FLOAT, DT_INT, REQ_GET, REQ_PUT, REQ_SIGNAL,
+from ._abi import (DT_DOUBLE, DT_FLOAT, DT_INT, REQ_GET, REQ_PUT, REQ_SIGNAL,
                    REQUEST_DTYPE)
 
 GOLDEN = np.uint64(0x9E3779B97F4A7C15)

@@ -151,7 +151,12 @@ int nvshmemx_batch_execute_percall(nvshmemx_batch *b, int mode, int reps, float 
  * NVSHMEMX_NOALLOC_MAX_CHUNKS requests and at most that many chunks of
  * cfg->chunk_bytes in total; larger batches are rejected with
  * NVSHMEMX_ERR_NOMEM and nothing is executed.  cfg NULL uses
- * nvshmemx_batch_default_config.
+ * nvshmemx_batch_default_config.  Every field of cfg is honoured as in
+ * nvshmemx_batch_execute (tma_stages > 0 runs the TMA-ring exec kernel,
+ * whose stages are shared memory, not scratch), except stream: stream mode
+ * keeps state across calls that the shared scratch cannot hold, so a cfg
+ * with stream != 0 is rejected with NVSHMEMX_ERR_INVALID.  As in the graph
+ * path, one invalid request stops the whole batch (nothing is executed).
  *
  * The first call on a device looks up the scratch array's device address
  * (cudaGetSymbolAddress, with that device current); make that first call

@@ -293,6 +293,35 @@ def test_bad_request_rejected_not_executed(shmem_factory):
     assert first_diff(heap_images(sh, npes, heap), om.heap) is None
 
 
+WRAP = (1 << 64) - 4  # offset + 8 wraps to 4: must be rejected, never executed
+
+
+@pytest.mark.parametrize("cfg", [CONFIGS[0], CONFIGS[4], STREAM])
+@pytest.mark.parametrize("field", ["src_off", "dst_off"])
+def test_wrapping_offsets_rejected(shmem_factory, cfg, field):
+    """An offset near 2^64 whose sum with the size wraps around is a bounds
+    error: the planner rejects it (graph path: nothing runs; stream mode:
+    that request alone is skipped) and no byte outside the valid requests
+    changes."""
+    npes, heap = 4, 1 << 20
+    sh, om = setup(shmem_factory, npes, heap)
+    good = c4_batch(seed=48, n=200, npes=npes, heap=heap, hi=4 << 10)
+    row = dict(src_off=0, dst_off=heap // 2 - 64, bytes=8, src_pe=1, dst_pe=2, op=REQ_PUT, dtype=0)
+    row[field] = WRAP
+    bad = requests([row])
+    reqs = np.concatenate([good[:100], bad, good[100:]])
+    with sh.batch(len(reqs), int(good["bytes"].sum()) + 64, 256) as b:
+        b.set_config(cfg)
+        b.upload(reqs)
+        with pytest.raises(Exception) as ei:
+            b.execute(1)
+        assert ei.value.code == ERR_BOUNDS
+    sh.status()
+    if cfg.get("stream"):
+        om.apply_requests(good)
+    assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+
+
 def test_empty_batch(shmem_factory):
     sh = shmem_factory(2, 1 << 20)
     with sh.batch(16, 1 << 16, 256) as b:

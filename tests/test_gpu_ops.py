@@ -5,7 +5,7 @@ barrier failure paths, which must end with NVSHMEMX_ERR_TIMEOUT, never hang."""
 import numpy as np
 import pytest
 
-from nvshmem_b200 import (DT_DOUBLE, DT_FLOAT, DT_INT, ERR_TIMEOUT, MODE_BLOCK,
+from nvshmem_b200 import (DT_DOUBLE, DT_FLOAT, DT_INT, ERR_INVALID, ERR_TIMEOUT, MODE_BLOCK,
                           MODE_BULK, MODE_THREAD, MODE_WARP, REQ_GET, REQ_PUT)
 from nvshmem_b200.traffic import c3_block
 from oracle.model import Model, checksum
@@ -180,6 +180,57 @@ def test_halo_bit_exact(shmem_factory, n, offload):
     assert sh.status() == 0
     om.halo(2, 2, 2, n, block_off, ghost_off, sig_off, 5)
     assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+
+
+@pytest.mark.parametrize("offload", [False, True], ids=["persistent", "offload_barrier"])
+def test_halo_benchmark_size_bit_exact(shmem_factory, offload):
+    """The benchmark's halo: 8 PEs, 256^3 float64 blocks (N(0,1), seed 3),
+    3 iterations, as many CTAs per PE as stay co-resident; every PE's heap
+    (block, ghosts, signal words and the bytes past them) is compared with the
+    oracle through per-PE checksums."""
+    npes, n, iters = 8, 256, 3
+    block = n * n * n * 8
+    ghosts = 6 * n * n * 8
+    heap = block + ghosts + 4096
+    sh = shmem_factory(npes, heap)
+    om = Model(npes, heap)
+    for pe in range(npes):
+        b = c3_block(n, pe)
+        sh.write(pe, 0, b)
+        om.heap[pe, :block] = b.view(np.uint8)
+        sh.memset(pe, block, 0, heap - block)
+    sh.halo(2, 2, 2, n, 0, block, block + ghosts, iters=iters, ctas_per_pe=0, offload=offload)
+    assert sh.status() == 0
+    om.halo(2, 2, 2, n, 0, block, block + ghosts, iters)
+    for pe in range(npes):
+        assert sh.checksum(pe, 0, heap) == checksum(om.heap[pe]), f"PE {pe}"
+
+
+def test_host_checks_reject_wrapping_arguments(shmem_factory):
+    """Offsets and counts whose sums or products wrap past 2^64 are invalid
+    arguments, refused on the host before any launch."""
+    sh = shmem_factory(8, 1 << 20)
+    huge = (1 << 64) - 8
+    with pytest.raises(Exception) as ei:
+        sh.alltoall(REQ_PUT, DT_INT, huge, 0, 64)
+    assert ei.value.code == ERR_INVALID
+    with pytest.raises(Exception) as ei:  # (nsets - 1) * set_stride wraps
+        sh.alltoall(REQ_PUT, DT_INT, 0, 4096, 64, rounds=2, nsets=3, set_stride=1 << 63)
+    assert ei.value.code == ERR_INVALID
+    with pytest.raises(Exception) as ei:  # n^3 * 8 wraps
+        sh.halo(2, 2, 2, 1 << 22, 0, 0, 0, 1, 1)
+    assert ei.value.code == ERR_INVALID
+    with pytest.raises(Exception) as ei:
+        sh.halo(2, 2, 2, 4, 0, 4096, huge, 1, 1)
+    assert ei.value.code == ERR_INVALID
+    with pytest.raises(Exception) as ei:
+        sh.wait_test(huge, 1, 1000)
+    assert ei.value.code == ERR_INVALID
+    assert sh.status() == 0
+    sh2 = shmem_factory(2, 1 << 20)
+    with pytest.raises(Exception) as ei:
+        sh2.pingpong(huge, 0, 0, 1)
+    assert ei.value.code == ERR_INVALID
 
 
 def test_wait_timeout_reports_and_returns(shmem_factory):

@@ -17,7 +17,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from nvshmem_b200 import ERR_NOMEM, REQ_PUT, _lib as L, default_batch_config
+from nvshmem_b200 import ERR_BOUNDS, ERR_INVALID, ERR_NOMEM, REQ_PUT, _lib as L, default_batch_config
 from nvshmem_b200.traffic import c4_batch
 from _util import heap_images, requests  # noqa: E402
 
@@ -36,9 +36,17 @@ def _noalloc(d, n, cfg=None):
                                                 ctypes.byref(cfg) if cfg is not None else None, None)
 
 
-def test_noalloc_matches_batch_execute_on_two_calls(shmem_factory):
+def _register_config():
+    cfg = default_batch_config()
+    cfg.tma_stages = 0
+    return cfg
+
+
+@pytest.mark.parametrize("which", ["default (TMA rings)", "register copy"])
+def test_noalloc_matches_batch_execute_on_two_calls(shmem_factory, which):
     npes, heap = 8, 8 << 20
     sh = shmem_factory(npes, heap)
+    cfg = default_batch_config() if which.startswith("default") else _register_config()
     for call, seed in enumerate((21, 22)):
         reqs = c4_batch(seed=seed, n=2000, npes=npes, heap=heap, hi=128 << 10)
         for pe in range(npes):
@@ -50,7 +58,7 @@ def test_noalloc_matches_batch_execute_on_two_calls(shmem_factory):
         for pe in range(npes):
             sh.fill_random(pe, 0, heap, 100 + call)
         d = _device_copy(reqs)
-        rc = _noalloc(d, len(reqs), default_batch_config())
+        rc = _noalloc(d, len(reqs), cfg)
         assert rc == 0, L.lib.nvshmemx_last_error_string()
         assert sh.status() == 0
         got = heap_images(sh, npes, heap)
@@ -75,5 +83,26 @@ def test_noalloc_rejects_batches_beyond_its_scratch(shmem_factory):
                     dict(src_off=0, dst_off=heap // 2, bytes=4 << 20, src_pe=1, dst_pe=0, op=REQ_PUT, dtype=0),
                     dict(src_off=0, dst_off=heap // 2 - 16, bytes=4, src_pe=1, dst_pe=1, op=REQ_PUT, dtype=0)])
     assert _noalloc(_device_copy(big), len(big), cfg) == ERR_NOMEM
+    sh.status()
+    assert np.array_equal(heap_images(sh, npes, heap), before)
+
+
+def test_noalloc_rejects_stream_mode_and_wrapping_offsets(shmem_factory):
+    """stream = 1 is refused (its state outlives a call, which the shared
+    scratch cannot hold), and an offset whose sum with the size wraps past
+    2^64 is a bounds error; in both cases no heap byte changes."""
+    npes, heap = 2, 1 << 20
+    sh = shmem_factory(npes, heap)
+    for pe in range(npes):
+        sh.fill_random(pe, 0, heap, 6)
+    before = heap_images(sh, npes, heap)
+    ok = requests([dict(src_off=0, dst_off=heap // 2, bytes=4096, src_pe=0, dst_pe=1, op=REQ_PUT, dtype=0)])
+    cfg = default_batch_config()
+    cfg.stream = 1
+    assert _noalloc(_device_copy(ok), 1, cfg) == ERR_INVALID
+    wrap = requests([dict(src_off=(1 << 64) - 4, dst_off=heap // 2, bytes=8, src_pe=0, dst_pe=1, op=REQ_PUT,
+                          dtype=0),
+                     dict(src_off=0, dst_off=heap // 2 + 64, bytes=4096, src_pe=0, dst_pe=1, op=REQ_PUT, dtype=0)])
+    assert _noalloc(_device_copy(wrap), len(wrap)) == ERR_BOUNDS
     sh.status()
     assert np.array_equal(heap_images(sh, npes, heap), before)
