@@ -226,6 +226,9 @@ def test_host_checks_reject_wrapping_arguments(shmem_factory):
     with pytest.raises(Exception) as ei:
         sh.wait_test(huge, 1, 1000)
     assert ei.value.code == ERR_INVALID
+    # the status word reports the first host-side refusal once, and no device
+    # error: nothing was launched
+    assert sh.status() == ERR_INVALID
     assert sh.status() == 0
     sh2 = shmem_factory(2, 1 << 20)
     with pytest.raises(Exception) as ei:
