@@ -950,6 +950,56 @@ static int ensure_graph(nvshmemx_batch *b, const nvshmemx_request *src) {
   return 0;
 }
 
+// ------------------------------------------------ grouped runs (picker.cu)
+// A run's plan or exec error, copied into the sticky word at byte 128 of the
+// control allocation unless that already holds one (first error wins).
+__global__ void sticky_status_kernel(const BatchCtl *ctl, int *sticky) {
+  if (threadIdx.x == 0 && ctl->status != 0 && sticky[0] == 0) {
+    sticky[0] = ctl->status;
+    sticky[1] = ctl->bad_request;
+  }
+}
+
+static int *sticky_word(nvshmemx_batch *b) {
+  return reinterpret_cast<int *>(reinterpret_cast<char *>(b->d_ctl) + 128);
+}
+
+namespace nvshm {
+cudaStream_t batch_stream(const nvshmemx_batch *b) { return b->stream; }
+nvshmemx_request *batch_device_requests(nvshmemx_batch *b) { return b->d_reqs; }
+int batch_capacity(const nvshmemx_batch *b) { return b->max_n; }
+int batch_min_chunk(const nvshmemx_batch *b) { return b->min_chunk; }
+
+int batch_enqueue_range(nvshmemx_batch *b, int first, int n, const nvshmemx_batch_config &cfg) {
+  if (first < 0 || n < 0 || first > b->max_n || n > b->max_n - first || cfg.stream != 0 || check_batch_config(cfg) ||
+      cfg.chunk_bytes < b->min_chunk)
+    return fail(NVSHMEMX_ERR_INVALID, "batch range run: bad range or configuration");
+  if (n == 0) return 0;
+  const nvshmemx_batch_config saved = b->cfg;
+  b->cfg = cfg;
+  int rc = check_cuda(cudaMemsetAsync(b->d_ctl, 0, sizeof(BatchCtl), b->stream), "cudaMemsetAsync");
+  if (!rc) rc = enqueue_piece(b, false, b->d_reqs + first, n, b->d_ctl, b->d_ctl, nullptr, 0, b->stream, kPlan | kExec);
+  b->cfg = saved;
+  if (!rc) {
+    sticky_status_kernel<<<1, 32, 0, b->stream>>>(b->d_ctl, sticky_word(b));
+    rc = check_cuda(cudaGetLastError(), "sticky status kernel");
+  }
+  return rc;
+}
+
+int batch_clear_sticky(nvshmemx_batch *b) {
+  return check_cuda(cudaMemsetAsync(sticky_word(b), 0, 8, b->stream), "cudaMemsetAsync(sticky)");
+}
+
+int batch_sticky_status(nvshmemx_batch *b, int *status, int *bad_request) {
+  int st[2] = {0, 0};
+  int rc = check_cuda(cudaMemcpy(st, sticky_word(b), 8, cudaMemcpyDeviceToHost), "read sticky status");
+  *status = st[0];
+  *bad_request = st[1];
+  return rc;
+}
+}  // namespace nvshm
+
 extern "C" {
 
 // The autotuner's best on the 64-PE / 100,000-request workload: per-warp TMA
@@ -985,7 +1035,7 @@ int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes
       (rc = check_cuda(cudaMalloc(&b->d_reqs_compact, (size_t)max_requests * sizeof(nvshmemx_request_compact)),
                        "cudaMalloc(compact reqs)")) ||
       (rc = check_cuda(cudaMalloc(&b->d_items, (size_t)b->cap * sizeof(WorkItem)), "cudaMalloc(items)")) ||
-      (rc = check_cuda(cudaMalloc(&b->d_ctl, 128), "cudaMalloc(ctl)")) ||
+      (rc = check_cuda(cudaMalloc(&b->d_ctl, 256), "cudaMalloc(ctl)")) ||
       (rc = check_cuda(cudaMallocHost(&b->h_reqs, (size_t)max_requests * sizeof(nvshmemx_request)),
                        "cudaMallocHost(reqs)")) ||
       (rc = check_cuda(cudaMallocHost(&b->h_status, 64), "cudaMallocHost(status)")) ||
@@ -1010,7 +1060,7 @@ int nvshmemx_batch_create(int max_requests, unsigned long long max_payload_bytes
   b->h_status_dev = static_cast<int *>(hs);
   // control block (BatchCtl or StreamCtl) and every work item's generation
   // tag start at zero; streaming generations start at 1
-  cudaMemset(b->d_ctl, 0, 128);
+  cudaMemset(b->d_ctl, 0, 256);
   cudaMemset(b->d_items, 0, (size_t)b->cap * sizeof(WorkItem));
   *out = b;
   return 0;

@@ -20,4 +20,19 @@ int check_batch_config(const nvshmemx_batch_config &c);
 // not start with its data in L2 (tuner.cu).
 int l2_flush(size_t bytes);
 
+// For the picker's grouped execution (picker.cu): b's stream, its
+// device-resident request array (room for batch_capacity requests), and an
+// enqueue (no graph, no wait) of zeroing + plan + exec of requests
+// [first, first + n) with configuration cfg.  A plan or exec error of the
+// run is kept in a status word that later runs do not clear; read it with
+// batch_sticky_status after the stream has finished, clear it with
+// batch_clear_sticky before the first run.
+cudaStream_t batch_stream(const nvshmemx_batch *b);
+nvshmemx_request *batch_device_requests(nvshmemx_batch *b);
+int batch_capacity(const nvshmemx_batch *b);
+int batch_min_chunk(const nvshmemx_batch *b);
+int batch_enqueue_range(nvshmemx_batch *b, int first, int n, const nvshmemx_batch_config &cfg);
+int batch_clear_sticky(nvshmemx_batch *b);
+int batch_sticky_status(nvshmemx_batch *b, int *status, int *bad_request);
+
 }  // namespace nvshm

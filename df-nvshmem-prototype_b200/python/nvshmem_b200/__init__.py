@@ -14,7 +14,8 @@ from ._abi import (CMP_EQ, CMP_GE, CMP_GT, CMP_LE, CMP_LT, CMP_NE, DT_DOUBLE,  #
                    ERR_INVALID, ERR_NOMEM, ERR_STATE, ERR_TIMEOUT, ERR_UNSUPPORTED, ERRORS_EXIT,
                    ERRORS_RETURN, MODE_BLOCK, MODE_BULK, MODE_THREAD, MODE_WARP, REQ_G, REQ_GET,
                    REQ_P, REQ_PUT, REQ_SIGNAL, REQUEST_COMPACT_DTYPE, REQUEST_DTYPE, SUCCESS,
-                   TRACE_DTYPE)
+                   TRACE_DTYPE, PICKED_GROUP_DTYPE, PATTERN_PAIRS, PATTERN_ALLTOALL, PATTERN_NEIGHBOR,
+                   PATTERN_RANDOM)
 
 # names backed by the shared library, resolved on first use
 _NATIVE = {"LIB_PATH": "_lib", "BatchConfig": "_lib", "ShmemError": "_lib",

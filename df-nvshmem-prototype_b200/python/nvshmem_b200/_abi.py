@@ -35,3 +35,9 @@ TRACE_DTYPE = np.dtype([
     ("block", "<u4"),
 ])
 assert TRACE_DTYPE.itemsize == 48
+
+# nvshmemx_picked_group (include/nvshmemx_picker.h)
+PICKED_GROUP_DTYPE = np.dtype([("first", "<i4"), ("count", "<i4"), ("variant", "<i4"), ("source", "<i4"),
+                               ("features", "<f4", (6,))])
+assert PICKED_GROUP_DTYPE.itemsize == 40
+PATTERN_PAIRS, PATTERN_ALLTOALL, PATTERN_NEIGHBOR, PATTERN_RANDOM = range(4)

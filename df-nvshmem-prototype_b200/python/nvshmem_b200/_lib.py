@@ -21,7 +21,8 @@ from ._abi import (  # noqa: F401  (re-exported)
     SUCCESS, ERR_INVALID, ERR_NOMEM, ERR_CUDA, ERR_STATE, ERR_TIMEOUT, ERR_BOUNDS, ERR_COOP, ERR_UNSUPPORTED,
     ERRORS_EXIT, ERRORS_RETURN, CMP_EQ, CMP_NE, CMP_GT, CMP_GE, CMP_LT, CMP_LE,
     REQ_PUT, REQ_GET, REQ_SIGNAL, REQ_P, REQ_G, DT_INT, DT_FLOAT, DT_DOUBLE, DT_WIDTH,
-    MODE_THREAD, MODE_WARP, MODE_BLOCK, MODE_BULK, REQUEST_DTYPE, REQUEST_COMPACT_DTYPE, TRACE_DTYPE)
+    MODE_THREAD, MODE_WARP, MODE_BLOCK, MODE_BULK, REQUEST_DTYPE, REQUEST_COMPACT_DTYPE, TRACE_DTYPE,
+    PICKED_GROUP_DTYPE, PATTERN_PAIRS, PATTERN_ALLTOALL, PATTERN_NEIGHBOR, PATTERN_RANDOM)
 
 
 class BatchConfig(ctypes.Structure):
@@ -133,6 +134,12 @@ _SIGS = {
     "nvshmemx_mlp_pick": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     "nvshmemx_variant_time": (c_int, [c_void_p, c_int, c_int, c_size_t, _P(c_float)]),
     "nvshmemx_variant_describe": (c_int, [c_int, _P(c_int), _P(BatchConfig)]),
+    "nvshmemx_picker_create": (c_int, [c_void_p, c_void_p, c_void_p, c_int, _P(c_void_p)]),
+    "nvshmemx_picker_destroy": (c_int, [c_void_p]),
+    "nvshmemx_picker_pick": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "nvshmemx_picker_table_pick": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
+    "nvshmemx_batch_execute_picked": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_int,
+                                              _P(c_int), _P(c_int), _P(c_float)]),
     # nvshmemx_tune.h
     "nvshmemx_tune_candidates": (c_int, [_P(BatchConfig), c_int, c_int]),
     "nvshmemx_tune_batch": (c_int, [c_void_p, _P(BatchConfig), c_int, c_int, c_size_t, _P(TuneResult),

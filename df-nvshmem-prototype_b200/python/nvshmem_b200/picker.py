@@ -11,9 +11,10 @@ Every class is executed with each of the 12 variants (per-call thread, warp,
 CTA, CTA-TMA; batch-engine shapes with register or TMA copies), L2 flushed
 before every run; the median device time per variant is one training row.
 The network (own CUDA forward/backward/Adam kernels) learns log2 time per
-variant from the class features; the picker takes the fastest prediction and
-falls back to the measured table's nearest class when the features leave
-the training range.  Regret = total time of the picked variants over the
+variant from the class features; the picker (nvshmemx_picker_*, in C) takes
+the fastest prediction and falls back to the measured table's nearest class
+when the features leave the training range.  Training classes cover all four
+patterns (the C1-C3 shapes and C4's random pairs).  Regret = total time of the picked variants over the
 exhaustive best, minus 1.
 
   python -m nvshmem_b200.picker sweep [--out tuned/variant_timings.npz]
@@ -147,9 +148,12 @@ def measure(classes, seed0: int, reps: int = 3, flush_bytes: int = 256 << 20, lo
     return T
 
 
-def sweep(out: str = DATA, n_train: int = 600, n_mixes: int = 20, per_mix: int = 8, reps: int = 3, log=print):
+TRAIN_PATTERNS = (0, 1, 2, 3)  # C1..C3 traffic shapes and C4's random pairs
+
+
+def sweep(out: str = DATA, n_train: int = 800, n_mixes: int = 20, per_mix: int = 8, reps: int = 3, log=print):
     t0 = time.time()
-    train = sample_classes(seed=2024, n=n_train, patterns=(0, 1, 2))  # C1..C3 traffic shapes
+    train = sample_classes(seed=2024, n=n_train, patterns=TRAIN_PATTERNS)
     mixes = [sample_classes(seed=s, n=per_mix, patterns=(0, 1, 2, 3)) for s in range(100, 100 + n_mixes)]
     held = [c for m in mixes for c in m]
     Tt = measure(train, 10_000, reps, log=log)
@@ -158,7 +162,8 @@ def sweep(out: str = DATA, n_train: int = 600, n_mixes: int = 20, per_mix: int =
              held_x=np.stack([features(**c) for c in held]), held_t=Th,
              mix_of=np.repeat(np.arange(n_mixes), per_mix),
              meta=json.dumps({"variants": VARIANT_NAMES, "reps": reps, "seconds": time.time() - t0,
-                              "train_seed": 2024, "mix_seeds": [100, 100 + n_mixes - 1]}))
+                              "train_seed": 2024, "train_patterns": list(TRAIN_PATTERNS),
+                              "mix_seeds": [100, 100 + n_mixes - 1]}))
     return out
 
 
@@ -231,44 +236,58 @@ def targets(T):
 
 
 class Picker:
-    """MLP picker with the measured table as fallback."""
+    """The library's run-time picker (nvshmemx_picker_*): the network's choice
+    while every feature lies inside the measured table's range, the table's
+    nearest class otherwise -- both decided in C, the same code that
+    nvshmemx_batch_execute_picked runs."""
 
     def __init__(self, train_x, train_t, seed=0):
-        self.tx = np.asarray(train_x, np.float32)
-        self.tt = np.asarray(train_t)
-        self.mean = self.tx.mean(0)
-        self.std = np.maximum(self.tx.std(0), 1e-3)
-        self.lo, self.hi = self.tx.min(0), self.tx.max(0)
+        self.tx = np.ascontiguousarray(train_x, np.float32)
+        self.tt = np.ascontiguousarray(train_t, np.float32)  # NaN: variant did not run
         self.mlp = MLP(seed)
-        self.mlp.set_normalization(self.mean, self.std)
+        self.h = c_void_p(0)
+        check(lib.nvshmemx_picker_create(self.mlp.h, self.tx.ctypes.data, self.tt.ctypes.data, len(self.tx),
+                                         byref(self.h)), "picker_create")
         self.curve = None
 
+    def close(self):
+        if self.h:
+            lib.nvshmemx_picker_destroy(self.h)
+            self.h = c_void_p(0)
+
+    def __del__(self):
+        self.close()
+
     def fit(self, epochs=400, batch=128, lr=2e-3, seed=1):
-        Y, M = targets(self.tt)
+        Y, M = targets(self.tt.astype(np.float64))
         self.curve = self.mlp.train(self.tx, Y, M, epochs, batch, lr, seed)
         return self.curve
 
     def table_pick(self, X):
-        """Best measured variant of the nearest training class."""
-        z = (np.asarray(X, np.float32) - self.mean) / self.std
-        zt = (self.tx - self.mean) / self.std
-        d = ((z[:, None, :] - zt[None, :, :]) ** 2).sum(-1)
-        nn = d.argmin(1)
-        return np.array([int(np.nanargmin(self.tt[i])) for i in nn]), nn
+        """Best measured variant of the nearest table class."""
+        X = np.ascontiguousarray(X, np.float32)
+        v = np.zeros(len(X), np.int32)
+        check(lib.nvshmemx_picker_table_pick(self.h, X.ctypes.data, len(X), v.ctypes.data), "picker_table_pick")
+        return v
 
     def pick(self, X):
-        """MLP choice; the table's where a feature leaves the training range."""
-        X = np.asarray(X, np.float32)
-        v, _ = self.mlp.pick(X)
-        out_of_range = np.any((X < self.lo - 1e-6) | (X > self.hi + 1e-6), axis=1)
-        tv, _ = self.table_pick(X)
-        return np.where(out_of_range, tv, v), out_of_range
+        """(variant, decided by the table) per feature row."""
+        X = np.ascontiguousarray(X, np.float32)
+        v = np.zeros(len(X), np.int32)
+        src = np.zeros(len(X), np.int32)
+        check(lib.nvshmemx_picker_pick(self.h, X.ctypes.data, len(X), v.ctypes.data, src.ctypes.data),
+              "picker_pick")
+        return v, src == 1
+
+
+def _chosen(T, picks):
+    return np.array([T[i, p] if np.isfinite(T[i, p]) else np.nanmax(T[i]) for i, p in enumerate(picks)])
 
 
 def regret(T, picks, mix_of):
     """Per mix: sum of picked times / sum of best times - 1."""
     best = np.nanmin(T, axis=1)
-    chosen = np.array([T[i, p] if np.isfinite(T[i, p]) else np.nanmax(T[i]) for i, p in enumerate(picks)])
+    chosen = _chosen(T, picks)
     out = []
     for m in np.unique(mix_of):
         sel = mix_of == m
@@ -276,13 +295,20 @@ def regret(T, picks, mix_of):
     return np.array(out)
 
 
+def subset_regret(T, picks, sel):
+    """Sum of picked times / sum of best times - 1 over the selected classes."""
+    if not np.any(sel):
+        return float("nan")
+    return float(_chosen(T, picks)[sel].sum() / np.nanmin(T, axis=1)[sel].sum() - 1.0)
+
+
 def evaluate(data: str = DATA, epochs=400, seed=0):
     d = np.load(data)
     pk = Picker(d["train_x"], d["train_t"], seed=seed)
     curve = pk.fit(epochs=epochs)
     hx, ht, mix = d["held_x"], d["held_t"], d["mix_of"]
-    mlp_v, oor = pk.pick(hx)
-    tab_v, _ = pk.table_pick(hx)
+    mlp_v, by_table = pk.pick(hx)
+    tab_v = pk.table_pick(hx)
     res = {
         "mlp": regret(ht, mlp_v, mix),
         "table": regret(ht, tab_v, mix),
@@ -291,9 +317,19 @@ def evaluate(data: str = DATA, epochs=400, seed=0):
     }
     summary = {k: {"mean_regret_pct": round(100 * float(v.mean()), 2), "max_regret_pct": round(100 * float(v.max()), 2)}
                for k, v in res.items()}
+    # the classes the network decided (every feature inside the table's
+    # range), on their own: the network's picks against the table's
+    net = ~by_table
+    summary["network_decided"] = {
+        "classes": int(net.sum()),
+        "network_regret_pct": round(100 * subset_regret(ht, mlp_v, net), 2),
+        "table_regret_pct": round(100 * subset_regret(ht, tab_v, net), 2)}
     summary["train_loss_first_last"] = [float(curve[0]), float(curve[-1])]
     summary["held_out_classes"] = int(len(hx))
-    summary["fallback_used"] = int(oor.sum())
+    summary["fallback_used"] = int(by_table.sum())
+    meta = json.loads(str(d["meta"])) if "meta" in d.files else {}
+    summary["train_patterns"] = meta.get("train_patterns", [0, 1, 2])
+    pk.close()
     return summary, res, pk
 
 
@@ -302,7 +338,7 @@ def main():
     ap.add_argument("cmd", choices=["sweep", "evaluate"])
     ap.add_argument("--out", default=DATA)
     ap.add_argument("--data", default=DATA)
-    ap.add_argument("--n-train", type=int, default=600)
+    ap.add_argument("--n-train", type=int, default=800)
     ap.add_argument("--reps", type=int, default=3)
     a = ap.parse_args()
     if a.cmd == "sweep":

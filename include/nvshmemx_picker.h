@@ -10,9 +10,11 @@
  *   (log2 bytes, element width, log2 alignment, log2 PEs, pattern id,
  *    log2 requests in flight)
  * and the picker takes the fastest prediction, falling back to the measured
- * table (nvshmemx_tune.h) when the inputs leave the range the network was
- * trained on.  The network is trained on the GPU by this library's own
- * forward, backward and Adam kernels.
+ * table of variant timings it was trained on when the inputs leave the range
+ * of that table (nvshmemx_picker_pick); nvshmemx_batch_execute_picked groups
+ * a request array and runs every group with its picked variant.  The
+ * network is trained on the GPU by this library's own forward, backward and
+ * Adam kernels.
  */
 #ifndef NVSHMEM_B200_NVSHMEMX_PICKER_H_
 #define NVSHMEM_B200_NVSHMEMX_PICKER_H_
@@ -60,6 +62,65 @@ int nvshmemx_mlp_train(nvshmemx_mlp *m, const float *X, const float *Y, const fl
 /* For each of n feature rows: the variant with the smallest predicted time
  * and the predicted gap to the runner-up (log2 units). */
 int nvshmemx_mlp_pick(nvshmemx_mlp *m, const float *X, int n, int *variant, float *margin);
+
+/* ---- picking at run time --------------------------------------------------
+ * A picker couples a trained network with the measured table it learned
+ * from: nt classes with features table_x[nt][6] and measured times
+ * table_t[nt][12] (ms; NaN or <= 0 where a variant did not run).  It sets
+ * the network's input normalisation to the table's per-feature mean and
+ * standard deviation (so create the picker before training the network) and
+ * keeps the per-feature range of the table as the range the network is
+ * trusted in.  The network must outlive the picker. */
+typedef struct nvshmemx_picker nvshmemx_picker;
+
+int nvshmemx_picker_create(nvshmemx_mlp *net, const float *table_x, const float *table_t, int nt,
+                           nvshmemx_picker **out);
+int nvshmemx_picker_destroy(nvshmemx_picker *p);
+
+/* For each of n feature rows: the network's fastest variant when every
+ * feature lies inside the table's range (source 0), else the best measured
+ * variant of the nearest table class -- Euclidean distance of the
+ * standardised features -- (source 1).  source may be NULL. */
+int nvshmemx_picker_pick(nvshmemx_picker *p, const float *X, int n, int *variant, int *source);
+
+/* The table's choice alone (nearest class's best measured variant). */
+int nvshmemx_picker_table_pick(nvshmemx_picker *p, const float *X, int n, int *variant);
+
+/* Pattern ids of the feature vector. */
+#define NVSHMEMX_PATTERN_PAIRS 0      /* PE pairs (put sweeps, ping-pong)     */
+#define NVSHMEMX_PATTERN_ALLTOALL 1   /* every PE to every other              */
+#define NVSHMEMX_PATTERN_NEIGHBOR 2   /* nearest neighbours on a PE grid      */
+#define NVSHMEMX_PATTERN_RANDOM 3     /* uniform random PE pairs              */
+
+/* One group of a picked execution. */
+typedef struct nvshmemx_picked_group {
+  int first;        /* index of its first request in the grouped order     */
+  int count;        /* requests in the group                               */
+  int variant;      /* variant that ran it (0..11)                          */
+  int source;       /* 0 network, 1 table fallback, 2 fixed (SIGNAL/P/G)    */
+  float features[NVSHMEMX_PICKER_NIN];
+} nvshmemx_picked_group;
+
+/* Executes n requests (a host array, any host memory) through the picker.
+ * Requests are validated on the host first (PEs, op, type, every range
+ * inside its slice, SIGNAL/P alignment); an invalid one fails the call with
+ * nothing executed.  PUT/GET requests are grouped by element width,
+ * relative source/destination alignment (4, 8 or 16 bytes) and size class
+ * (floor(log2 bytes)); each group's features are (log2 of its mean size,
+ * width, log2 alignment, log2 PE count, `pattern`, log2 of its request
+ * count), and the picker chooses its variant (network, or table outside the
+ * trained range).  SIGNAL, P and G requests form one group run by the batch
+ * engine's default configuration.  Groups that chose the same variant run
+ * together: one per-call launch or one batch run per variant, in one stream
+ * order on the batch's stream; the requests occupy the batch's device
+ * request array (so n <= its max_requests) in grouped order.  groups
+ * (room for max_groups entries, may be NULL) receives the groups, *ngroups
+ * their count; *out_status the first execution error (0: every request
+ * done); *out_ms the device time from the request copy to the end of the
+ * last run. */
+int nvshmemx_batch_execute_picked(nvshmemx_batch *b, nvshmemx_picker *p, const nvshmemx_request *reqs, int n,
+                                  int pattern, nvshmemx_picked_group *groups, int max_groups, int *ngroups,
+                                  int *out_status, float *out_ms);
 
 /* Execution of variant v (0..11) on b's uploaded requests, with L2 flushed
  * before each of `reps` runs; *out_ms = median device time. */

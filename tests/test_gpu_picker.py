@@ -76,4 +76,8 @@ def test_picker_beats_the_methods_without_it():
     assert mlp < res["default_variant"].mean()
     assert mlp < res["percall_thread"].mean()
     assert mlp <= res["table"].mean() + 0.02
+    # on the classes the network decides itself, it beats the table
+    nd = summary["network_decided"]
+    assert nd["classes"] > 0.5 * summary["held_out_classes"]
+    assert nd["network_regret_pct"] < nd["table_regret_pct"]
     assert summary["train_loss_first_last"][1] < 0.5 * summary["train_loss_first_last"][0]
