@@ -396,6 +396,52 @@ def run_c5_picker():
     return summary
 
 
+def run_c4_picked(steps, flush):
+    """The C4 batch through nvshmemx_batch_execute_picked: host requests
+    grouped by size class, width and alignment, a variant picked per group by
+    the trained network (the measured table outside its range), each variant
+    run once; L2 flushed before each step.  Checked against the batch engine's
+    result (per-PE heap checksums) and timed beside it."""
+    import numpy as np
+    from nvshmem_b200 import PATTERN_RANDOM, Shmem, picker, requests_bytes
+    from nvshmem_b200.traffic import c4_batch
+    if not os.path.exists(picker.DATA):
+        return {"unavailable": "no variant timings measured"}
+    d = np.load(picker.DATA)
+    pk = picker.Picker(d["train_x"], d["train_t"], seed=0)
+    pk.fit(epochs=400)
+    reqs = c4_batch(**C4)
+    alg = requests_bytes(reqs)
+    with Shmem(C4["npes"], C4["heap"]) as sh:
+        for pe in range(C4["npes"]):
+            sh.fill_random(pe, 0, C4["heap"], 44)
+        with sh.batch(len(reqs), int(reqs["bytes"].sum()), 256) as b:
+            b.upload(reqs)
+            b.execute(1)
+            want = [sh.checksum(pe, 0, C4["heap"]) for pe in range(C4["npes"])]
+            ms = []
+            for i in range(steps + 1):
+                flush()
+                st, t, groups = b.execute_picked(pk, reqs, PATTERN_RANDOM)
+                assert st == 0, f"picked execution status {st}"
+                if i:
+                    ms.append(t)
+            got = [sh.checksum(pe, 0, C4["heap"]) for pe in range(C4["npes"])]
+            assert got == want, "picked execution differs from the batch engine"
+        assert sh.status() == 0
+    pk.close()
+    per_variant = {}
+    for g in groups:
+        k = picker.VARIANT_NAMES[int(g["variant"])]
+        per_variant[k] = per_variant.get(k, 0) + int(g["count"])
+    med = statistics.median(ms)
+    return {"GBps": round(alg / (med / 1e3) / 1e9, 1), "ms": round(med, 4), "groups": int(len(groups)),
+            "decided_by": {"network": int((groups["source"] == 0).sum()), "table": int((groups["source"] == 1).sum()),
+                           "fixed": int((groups["source"] == 2).sum())},
+            "requests_per_variant": per_variant,
+            "timing": "device time from the host-to-device request copy to the end of the last run"}
+
+
 def cpu_latency():
     from oracle import model as om
     if not os.path.exists(om.HOST_BENCH):
@@ -507,6 +553,7 @@ def run_gpu(args, rank, world, local):
             out["c2_alltoall_sweep"] = run_c2_sweep(peak)
             out["c3_halo"] = run_c3_halo(peak)
             out["c5_picker_regret"] = run_c5_picker()
+            out["c4_picked"] = run_c4_picked(max(3, args.steps // 4), flush)
     clocks = sampler.summary()
 
     value = world * alg * args.steps / t_batch / 1e9

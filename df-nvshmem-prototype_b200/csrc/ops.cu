@@ -270,6 +270,106 @@ __global__ void barrier_latency_kernel(int iters, int counted, long long *cycles
 }
 
 // -------------------------------------------------------------- C2 all-to-all
+// A CTA's share of one all-to-all round, [b, e) of the PE's (npes-1) *
+// `bytes` outgoing (put) or incoming (get) bytes, streamed by one thread
+// through one TMA ring of kA2aStages stages: the ring runs across message
+// boundaries, so a share that spans two messages is loaded and stored
+// without draining the ring between them (a cooperative bulk copy per
+// message fills and drains its ring once per message).  Every chunk stays
+// inside one message; all addresses are 16-byte aligned (the caller checks).
+// Shared memory: 8 mbarriers, the destination and length of each stage's
+// chunk (256 bytes), then the stages.  Stage reuse lags one store behind,
+// as in bulk_copy_1t.  Returns false if an mbarrier wait passed `deadline`.
+constexpr unsigned kA2aStages = 6;
+
+// Where message k of the share starts: its destination and source.
+__device__ __forceinline__ void a2a_message(const Cfg &c, int op, int pe, unsigned long long so, unsigned long long ro,
+                                            unsigned long long bytes, unsigned long long k, char **dst,
+                                            const char **src) {
+  const int q = (pe + 1 + (int)k) % c.npes;
+  if (op == NVSHMEMX_REQ_PUT) {
+    *dst = xlate(c, c.arena + ro + (unsigned long long)pe * bytes, q);
+    *src = slice_ptr(c, pe, so + (unsigned long long)q * bytes);
+  } else {
+    *dst = slice_ptr(c, pe, ro + (unsigned long long)q * bytes);
+    *src = xlate(c, c.arena + so + (unsigned long long)pe * bytes, q);
+  }
+}
+
+// The issuing thread walks the share message by message (one division at
+// the start, none per chunk): a chunk costs it a few instructions, since at
+// tens of GB/s per CTA a 10 KiB chunk leaves it a few hundred cycles.
+__device__ __forceinline__ bool a2a_stream_1t(const Cfg &c, char *smem, unsigned smem_bytes, int op, int pe,
+                                              unsigned long long so, unsigned long long ro, unsigned long long bytes,
+                                              unsigned long long b, unsigned long long e,
+                                              unsigned long long deadline) {
+  if (b >= e) return true;
+  const unsigned S = kA2aStages;
+  unsigned long long *mbar = reinterpret_cast<unsigned long long *>(smem);
+  unsigned long long *sdst = reinterpret_cast<unsigned long long *>(smem + 64);
+  unsigned *slen = reinterpret_cast<unsigned *>(smem + 128);
+  char *buf = smem + 256;
+  const unsigned SB = ((smem_bytes - 256) / S) & ~127u;
+  for (unsigned s = 0; s < S; ++s) mbar_init(mbar + s, 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  unsigned long long k = b / bytes, off = b - k * bytes, left = e - b;
+  char *dbase;
+  const char *sbase;
+  a2a_message(c, op, pe, so, ro, bytes, k, &dbase, &sbase);
+  unsigned issued = 0, stored = 0;
+  while (issued < S && left) {
+    unsigned long long len = bytes - off;
+    if (len > left) len = left;
+    if (len > SB) len = SB;
+    sdst[issued] = (unsigned long long)(dbase + off);
+    slen[issued] = (unsigned)len;
+    mbar_expect_tx(mbar + issued, (unsigned)len);
+    bulk_g2s(buf + (size_t)issued * SB, sbase + off, (unsigned)len, mbar + issued);
+    ++issued;
+    off += len;
+    left -= len;
+    if (off == bytes && left) {
+      off = 0;
+      a2a_message(c, op, pe, so, ro, bytes, ++k, &dbase, &sbase);
+    }
+  }
+  bool ok = true;
+  while (stored < issued) {
+    const unsigned s = stored % S;
+    if (!mbar_wait(mbar + s, (stored / S) & 1u, deadline)) {
+      ok = false;
+      break;
+    }
+    bulk_s2g(reinterpret_cast<void *>(sdst[s]), buf + (size_t)s * SB, slen[s]);
+    bulk_commit();
+    // refill the stage the previous store read, not this one (see bulk_copy_1t)
+    if (stored >= 1 && left) {
+      bulk_wait_read1();
+      const unsigned ps = (stored - 1) % S;
+      unsigned long long len = bytes - off;
+      if (len > left) len = left;
+      if (len > SB) len = SB;
+      sdst[ps] = (unsigned long long)(dbase + off);
+      slen[ps] = (unsigned)len;
+      mbar_expect_tx(mbar + ps, (unsigned)len);
+      bulk_g2s(buf + (size_t)ps * SB, sbase + off, (unsigned)len, mbar + ps);
+      ++issued;
+      off += len;
+      left -= len;
+      if (off == bytes && left) {
+        off = 0;
+        a2a_message(c, op, pe, so, ro, bytes, ++k, &dbase, &sbase);
+      }
+    }
+    ++stored;
+  }
+  bulk_wait_all();
+  if (ok)
+    for (unsigned s = 0; s < S; ++s) mbar_inval(mbar + s);
+  return ok;
+}
+
 // Message k (0..npes-2) of PE p goes to / comes from peer q = (p+1+k) % npes.
 // For the cooperative modes the PE's (npes-1)*bytes are cut into one
 // contiguous, 16-byte-rounded segment per caller unit (warp or CTA), so every
@@ -315,6 +415,14 @@ __global__ void alltoall_kernel(Cfg c, int op, int dtype, unsigned long long sen
           else nvshmem_double_get((double *)dst, (double *)sym, len, q);
         }
       }
+    } else if (MODE == NVSHMEMX_MODE_BULK && ((bytes | so | ro) & 15) == 0) {
+      // one ring per CTA across its whole share of the round
+      const unsigned long long seg = (((total + nunits - 1) / nunits) + 15) & ~15ull;
+      const unsigned long long b = unit * seg;
+      const unsigned long long e = b + seg < total ? b + seg : total;
+      if (threadIdx.x == 0 && b < e &&
+          !a2a_stream_1t(c, smem, bulk_smem, op, pe, so, ro, bytes, b, e, gtimer() + (unsigned long long)c.wait_timeout_ns))
+        record_error(c, NVSHMEMX_ERR_TIMEOUT, -2);
     } else {
       const unsigned long long seg = (((total + nunits - 1) / nunits) + 15) & ~15ull;
       unsigned long long b = unit * seg;

@@ -7,7 +7,9 @@
 // network is not trusted outside the data it has seen).
 // nvshmemx_batch_execute_picked applies it to a request array: it groups
 // like requests, picks a variant per group, and runs the groups -- those
-// that chose the same variant together -- on the batch's stream.
+// that chose the same variant together: batch-engine shapes one after the
+// other on the batch's stream, per-call modes each on a stream of its own
+// beside them.
 //
 // The reference has one transfer method, the calling thread's scalar loop
 // (nvshmem_device.cu:498-500); every variant here gives the same heap
@@ -34,6 +36,10 @@ bool measured(float t) { return t > 0.f && isfinite(t); }
 
 struct nvshmemx_picker {
   nvshmemx_mlp *net = nullptr;
+  // picked execution: one stream per per-call mode (those runs overlap the
+  // batch runs and each other), and the events that fork and join them
+  cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev_copied = nullptr, ev_done[4] = {nullptr, nullptr, nullptr, nullptr};
   int nt = 0;
   std::vector<float> tx, tt;  // nt x kNin features, nt x kNv times (ms)
   float mean[kNin], sd[kNin], lo[kNin], hi[kNin];
@@ -101,9 +107,14 @@ int nvshmemx_picker_create(nvshmemx_mlp *net, const float *table_x, const float 
     p->lo[k] = lo;
     p->hi[k] = hi;
   }
-  const int rc = nvshmemx_mlp_set_normalization(net, p->mean, p->sd);
+  int rc = nvshmemx_mlp_set_normalization(net, p->mean, p->sd);
+  if (!rc) rc = check_cuda(cudaEventCreateWithFlags(&p->ev_copied, cudaEventDisableTiming), "cudaEventCreate");
+  for (int m = 0; m < 4 && !rc; ++m) {
+    rc = check_cuda(cudaStreamCreateWithFlags(&p->aux[m], cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!rc) rc = check_cuda(cudaEventCreateWithFlags(&p->ev_done[m], cudaEventDisableTiming), "cudaEventCreate");
+  }
   if (rc) {
-    delete p;
+    nvshmemx_picker_destroy(p);
     return rc;
   }
   *out = p;
@@ -111,6 +122,15 @@ int nvshmemx_picker_create(nvshmemx_mlp *net, const float *table_x, const float 
 }
 
 int nvshmemx_picker_destroy(nvshmemx_picker *p) {
+  if (!p) return 0;
+  for (int m = 0; m < 4; ++m) {
+    if (p->aux[m]) {
+      cudaStreamSynchronize(p->aux[m]);
+      cudaStreamDestroy(p->aux[m]);
+    }
+    if (p->ev_done[m]) cudaEventDestroy(p->ev_done[m]);
+  }
+  if (p->ev_copied) cudaEventDestroy(p->ev_copied);
   delete p;
   return 0;
 }
@@ -277,8 +297,10 @@ extern "C" int nvshmemx_batch_execute_picked(nvshmemx_batch *b, nvshmemx_picker 
     rc = check_cuda(cudaMemcpyAsync(d, perm.data(), (size_t)n * sizeof(nvshmemx_request), cudaMemcpyHostToDevice, st),
                     "cudaMemcpyAsync(requests)");
   if (!rc) rc = batch_clear_sticky(b);
+  if (!rc) rc = check_cuda(cudaEventRecord(p->ev_copied, st), "cudaEventRecord");
   nvshmemx_batch_config own;
   nvshmemx_batch_get_config(b, &own);
+  bool used[4] = {false, false, false, false};
   for (size_t k = 0; k < gs.size() && !rc;) {
     size_t e = k;
     int count = 0;
@@ -287,7 +309,12 @@ extern "C" int nvshmemx_batch_execute_picked(nvshmemx_batch *b, nvshmemx_picker 
     nvshmemx_batch_config c;
     nvshmemx_variant_describe(gs[k].variant, &mode, &c);
     if (mode >= 0) {
-      rc = launch_exec_requests(mode, d + first[k], count, st);
+      // a per-call run on its own stream, beside the batch runs (requests of
+      // one call touch disjoint bytes, so the runs may overlap)
+      rc = check_cuda(cudaStreamWaitEvent(p->aux[mode], p->ev_copied, 0), "cudaStreamWaitEvent");
+      if (!rc) rc = launch_exec_requests(mode, d + first[k], count, p->aux[mode]);
+      if (!rc) rc = check_cuda(cudaEventRecord(p->ev_done[mode], p->aux[mode]), "cudaEventRecord");
+      used[mode] = true;
     } else {
       // a shape whose chunk is below the batch's smallest chunk would not
       // fit its chunk table: run it with the batch's own configuration
@@ -296,6 +323,11 @@ extern "C" int nvshmemx_batch_execute_picked(nvshmemx_batch *b, nvshmemx_picker 
     }
     k = e;
   }
+  for (int m = 0; m < 4; ++m)
+    if (used[m]) {
+      const int wr = check_cuda(cudaStreamWaitEvent(st, p->ev_done[m], 0), "cudaStreamWaitEvent");
+      if (!rc) rc = wr;
+    }
   if (!rc) rc = check_cuda(cudaEventRecord(e1, st), "cudaEventRecord");
   if (!rc) rc = check_cuda(cudaStreamSynchronize(st), "batch_execute_picked");
   float ms = 0;

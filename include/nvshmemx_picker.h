@@ -111,8 +111,11 @@ typedef struct nvshmemx_picked_group {
  * count), and the picker chooses its variant (network, or table outside the
  * trained range).  SIGNAL, P and G requests form one group run by the batch
  * engine's default configuration.  Groups that chose the same variant run
- * together: one per-call launch or one batch run per variant, in one stream
- * order on the batch's stream; the requests occupy the batch's device
+ * together: one batch run per batch-engine shape, one after the other on the
+ * batch's stream, and one launch per per-call mode, each on a stream of the
+ * picker's own, beside the batch runs (the requests of one call touch
+ * disjoint bytes); the call returns when all are done.  The requests occupy
+ * the batch's device
  * request array (so n <= its max_requests) in grouped order.  groups
  * (room for max_groups entries, may be NULL) receives the groups, *ngroups
  * their count; *out_status the first execution error (0: every request
