@@ -272,46 +272,60 @@ def run_c1_sweep():
     return out
 
 
+C2_SIZES = [8 << k for k in range(26)]  # 8 B .. 256 MiB
+C2_TYPES = ((0, "int32"), (1, "float32"), (2, "float64"))
+
+
 def run_c2_sweep(peak, only_size=0):
-    """C2 all-to-all on 8 PEs across message sizes and element types: each
-    round every PE puts (or gets) one message to (from) each of the 7 others,
-    then quiet + device barrier; buffer sets rotate so large working sets
-    exceed 2x L2.  Bit-exactness is checked on the device after each size."""
-    from nvshmem_b200 import DT_DOUBLE, DT_FLOAT, DT_INT, MODE_BULK, REQ_GET, REQ_PUT, Shmem
+    """C2 all-to-all on 8 PEs, every message size from 8 B to 256 MiB in
+    powers of two, for int32, float32 and float64 payloads (random bits from
+    seed 1): each round every PE puts (or gets) one message to (from) each of
+    the 7 others through the CTA-wide TMA ring form (18 CTAs per PE), then
+    quiet + device barrier; buffer sets rotate so that large working sets
+    exceed 2x L2.  Below 1 MiB a round is mostly its fixed cost, reported as
+    us per round.  Every received message is compared with its source on the
+    device after each size.  The prototype's structure (a launch per round +
+    the host's nvshmem_barrier_all) is timed beside it on float32 at six
+    sizes."""
+    from nvshmem_b200 import MODE_BULK, REQ_GET, REQ_PUT, Shmem
     out = {}
-    plan = [(8, DT_INT), (512, DT_FLOAT), (32 << 10, DT_DOUBLE), (1 << 20, DT_FLOAT), (16 << 20, DT_INT),
-            (256 << 20, DT_DOUBLE)]
-    if only_size:
-        plan = [(b, d) for b, d in plan if b == only_size] or [(only_size, DT_FLOAT)]
-    for nbytes, dt in plan:
+    sizes = [only_size] if only_size else C2_SIZES
+    host_sizes = {8, 512, 32 << 10, 1 << 20, 16 << 20, 256 << 20}
+    for nbytes in sizes:
         nsets = max(1, min(8, (512 << 20) // (2 * 8 * 8 * nbytes)))
-        heap = 2 * 8 * nbytes * nsets
-        heap = max(heap, 1 << 20)
+        heap = max(2 * 8 * nbytes * nsets, 1 << 20)
         rounds = max(nsets, min(400, int(4e9 // max(112 * nbytes, 1))))
+        row = {}
         with Shmem(8, heap) as sh:
             for pe in range(8):
                 sh.fill_random(pe, 0, heap, 1)
-            row = {}
-            for op, name in ((REQ_PUT, "put"), (REQ_GET, "get")):
-                kw = dict(rounds=rounds, nsets=nsets, set_stride=16 * nbytes, mode=MODE_BULK, ctas_per_pe=18)
-                sh.alltoall(op, dt, 0, 8 * nbytes, nbytes, **dict(kw, rounds=nsets))
-                ms = sh.alltoall(op, dt, 0, 8 * nbytes, nbytes, **kw)
-                gbs = 2 * 8 * 7 * nbytes * rounds / (ms / 1e3) / 1e9
-                row[name] = {"GBps": round(gbs, 1), "frac": round(gbs / peak, 3), "us_per_round": round(1e3 * ms / rounds, 2)}
-            # the prototype's structure: a launch per round, then the host's
-            # nvshmem_barrier_all (device synchronisation + host barrier)
-            kw = dict(rounds=min(rounds, 50), nsets=nsets, set_stride=16 * nbytes, mode=MODE_BULK, ctas_per_pe=18,
-                      host_rounds=True)
-            ms = sh.alltoall(REQ_PUT, dt, 0, 8 * nbytes, nbytes, **kw)
-            gbs = 2 * 8 * 7 * nbytes * kw["rounds"] / (ms / 1e3) / 1e9
-            row["put_host_rounds"] = {"GBps": round(gbs, 1), "frac": round(gbs / peak, 3),
-                                      "us_per_round": round(1e3 * ms / kw["rounds"], 2)}
+            for dt, tname in C2_TYPES:
+                cell = {}
+                for op, name in ((REQ_PUT, "put"), (REQ_GET, "get")):
+                    kw = dict(rounds=rounds, nsets=nsets, set_stride=16 * nbytes, mode=MODE_BULK, ctas_per_pe=18)
+                    sh.alltoall(op, dt, 0, 8 * nbytes, nbytes, **dict(kw, rounds=nsets))
+                    ms = sh.alltoall(op, dt, 0, 8 * nbytes, nbytes, **kw)
+                    gbs = 2 * 8 * 7 * nbytes * rounds / (ms / 1e3) / 1e9
+                    cell[name] = {"GBps": round(gbs, 1), "frac": round(gbs / peak, 3),
+                                  "us_per_round": round(1e3 * ms / rounds, 2)}
+                row[tname] = cell
+            if nbytes in host_sizes:
+                kw = dict(rounds=min(rounds, 50), nsets=nsets, set_stride=16 * nbytes, mode=MODE_BULK,
+                          ctas_per_pe=18, host_rounds=True)
+                ms = sh.alltoall(REQ_PUT, 1, 0, 8 * nbytes, nbytes, **kw)
+                gbs = 2 * 8 * 7 * nbytes * kw["rounds"] / (ms / 1e3) / 1e9
+                row["put_host_rounds_float32"] = {"GBps": round(gbs, 1), "frac": round(gbs / peak, 3),
+                                                  "us_per_round": round(1e3 * ms / kw["rounds"], 2)}
             for p in range(8):
                 for q in range(8):
                     if p != q:
                         assert sh.compare(q, 8 * nbytes + p * nbytes, p, q * nbytes, nbytes) == 0
             assert sh.status() == 0
-        out[f"{nbytes}B_dt{dt}"] = row
+        out[f"{nbytes}B"] = row
+    big = [c["frac"] for k, r in out.items() if int(k[:-1]) >= (1 << 20)
+           for t, cell in r.items() if t in ("int32", "float32", "float64") for c in cell.values()]
+    if big:
+        out["min_frac_1MiB_and_up"] = min(big)
     return out
 
 
@@ -381,10 +395,21 @@ def run_c3_halo(peak, iters=100):
         ms_off = sh.halo(2, 2, 2, n, 0, block, sig, iters, 0, offload=True)
         assert sh.status() == 0
         check("offload")
+        # the x faces' scattered reads alone (one 8-byte element per 2 KiB
+        # row, both faces of all 8 PEs at once): the best of a few grid sizes
+        gather = min(sh.strided_read(0, (n - 1) * 8, 2, n * n, 8 * n, cp, 50) / 50 for cp in (18, 37, 74, 148))
     face_bytes = 8 * 6 * n * n * 8
-    return {"us_per_iter": round(1e3 * ms / iters, 2), "face_GBps": round(2 * face_bytes * iters / (ms / 1e3) / 1e9, 1),
+    us = 1e3 * ms / iters
+    # ceiling of one iteration's data movement: the x-face gather as measured
+    # above, plus the four contiguous faces (read + write) and the x faces'
+    # contiguous stores at the copy peak; synchronisation is not included
+    contig_us = (8 * 4 * n * n * 8 * 2 + 8 * 2 * n * n * 8) / (peak * 1e3)
+    ceiling_us = 1e3 * gather + contig_us
+    return {"us_per_iter": round(us, 2), "face_GBps": round(2 * face_bytes * iters / (ms / 1e3) / 1e9, 1),
             "iters": iters, "n": n, "ctas_per_pe": "as many as stay co-resident",
             "offload_barrier_us_per_iter": round(1e3 * ms_off / iters, 2),
+            "x_face_gather_ceiling_us": round(1e3 * gather, 2), "contiguous_faces_at_peak_us": round(contig_us, 2),
+            "frac_of_gather_ceiling": round(ceiling_us / us, 3),
             "bit_exact": "every ghost face and signal word of all 8 PEs after each timed run"}
 
 

@@ -485,6 +485,40 @@ __device__ __forceinline__ void halo_row_put(const Cfg &c, double *dst_sym, cons
   if (c.trace && lane == 0) trace_rec(c, NVSHMEMX_TRACE_PUT_INT, src, dst, bytes, pe, t0, gtimer());
 }
 
+// One x-face row: n doubles at stride n (src[k * n]) to n contiguous doubles
+// at dst_sym on PE pe, with the checks of nvshmem_double_p made once for the
+// row.  The gather is bound by DRAM access latency (every element is in its
+// own row of the block), so each lane keeps 8 loads in flight, read through
+// the non-coherent path without L1 allocation (the block is not written
+// during the exchange), before storing them; stores are relaxed, ordered by
+// the quiet that follows the faces.
+__device__ __forceinline__ void halo_xrow_put(const Cfg &c, double *dst_sym, const double *src, int n, int pe,
+                                              unsigned lane) {
+  const unsigned long long bytes = (unsigned long long)n * 8ull;
+  if (!check_remote(c, dst_sym, bytes, pe) || !check_local(c, src, (unsigned long long)(n - 1) * bytes + 8)) return;
+  unsigned long long *dst = reinterpret_cast<unsigned long long *>(xlate(c, dst_sym, pe));
+  const unsigned long long *s = reinterpret_cast<const unsigned long long *>(src);
+  const long long stride = n;
+  if (c.trace && lane == 0) {
+    const unsigned long long t = gtimer();
+    trace_rec(c, NVSHMEMX_TRACE_PUT_DOUBLE, src, dst, bytes, pe, t, t);
+  }
+  for (int k0 = 0; k0 < n; k0 += 256) {
+    unsigned long long v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int k = k0 + u * 32 + (int)lane;
+      if (k < n)
+        asm volatile("ld.global.nc.L1::no_allocate.b64 %0, [%1];" : "=l"(v[u]) : "l"(s + k * stride));
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int k = k0 + u * 32 + (int)lane;
+      if (k < n) st_relaxed_b64(dst + k, v[u]);
+    }
+  }
+}
+
 __global__ void __launch_bounds__(256, 4) halo_kernel(Cfg c, int px, int py, int pz, int n, unsigned long long block_off,
                             unsigned long long ghost_off, unsigned long long sig_off, int iters, int it0,
                             int device_barrier) {
@@ -503,9 +537,10 @@ __global__ void __launch_bounds__(256, 4) halo_kernel(Cfg c, int px, int py, int
                                (unsigned long long)j * n * 8ull);
       if (d < 2) {
         // x face: element (z=j, y=k) sits at blk[(j*n + k)*n + x0]; gather
-        // with stride n and store each double remotely
+        // with stride n (one 8-byte element per n*8-byte row) and store the
+        // row contiguously on the neighbour
         const int x0 = (d & 1) ? n - 1 : 0;
-        for (int k = lane; k < n; k += 32) nvshmem_double_p(dst + k, blk[((long long)j * n + k) * n + x0], nb);
+        halo_xrow_put(c, dst, blk + (long long)j * n * n + x0, n, nb, lane);
       } else if (d < 4) {
         // y face: row j is z=j, contiguous in x
         const int y0 = (d & 1) ? n - 1 : 0;
@@ -526,6 +561,41 @@ __global__ void __launch_bounds__(256, 4) halo_kernel(Cfg c, int px, int py, int
     }
     if (device_barrier) nvshmemx_barrier_all_ep((unsigned long long)it);
   }
+}
+
+// ------------------------------------------------ strided-read ceiling
+// What the halo's x faces cost at best: every PE reads nsets x rows 8-byte
+// elements, element i of set t at slice offset off + t * set_off +
+// i * stride, with ctas_per_pe CTAs per PE and 8 loads in flight per lane
+// (the access pattern of halo_xrow_put without its stores), and adds them
+// into one word per warp so that nothing is optimised away.
+__global__ void __launch_bounds__(256) strided_read_kernel(Cfg c, unsigned long long off, unsigned long long set_off,
+                                                           int nsets, unsigned long long rows,
+                                                           unsigned long long stride, unsigned long long *sink) {
+  const int pe = blockIdx.y;
+  const char *base = slice_ptr(c, pe, off);
+  const unsigned long long total = (unsigned long long)nsets * rows;
+  const unsigned long long nthr = (unsigned long long)gridDim.x * blockDim.x;
+  const unsigned long long t0 = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long acc = 0;
+  for (unsigned long long i0 = t0; i0 < total; i0 += 8 * nthr) {
+    unsigned long long v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const unsigned long long i = i0 + (unsigned long long)u * nthr;
+      v[u] = 0;
+      if (i < total) {
+        const unsigned long long set = i / rows, row = i - set * rows;
+        const char *p = base + set * set_off + row * stride;
+        asm volatile("ld.global.nc.L1::no_allocate.b64 %0, [%1];" : "=l"(v[u]) : "l"(p));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc += v[u];
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(sink, acc);
 }
 
 // ------------------------------------------------------- failure detection
@@ -904,6 +974,29 @@ int nvshmemx_op_halo_offload(int px, int py, int pz, int n, size_t block_off, si
   float ms = t.ms();
   if (out_ms) *out_ms = ms;
   return check_cuda(cudaDeviceSynchronize(), "halo_offload");
+}
+
+int nvshmemx_op_strided_read(size_t off, size_t set_off, int nsets, size_t rows, size_t stride, int ctas_per_pe,
+                             int iters, float *out_ms) {
+  int rc;
+  if ((rc = need_started())) return rc;
+  const Runtime &r = rt();
+  size_t span = 0, last = 0;
+  if (nsets < 1 || ctas_per_pe < 1 || iters < 1 || rows < 1 || stride < 8 || (off | set_off | stride) % 8 ||
+      !mul_ok(rows - 1, stride, &span) || !mul_ok((size_t)(nsets - 1), set_off, &last) ||
+      !range_ok(last, span + 8, r.heap_bytes) || !range_ok(off, last + span + 8, r.heap_bytes))
+    return fail(NVSHMEMX_ERR_INVALID, "strided_read: bad arguments or elements outside the heap");
+  unsigned long long *sink = (unsigned long long *)g_out_buf.get(64);
+  if (!sink) return fail(NVSHMEMX_ERR_NOMEM, "strided_read scratch");
+  EventTimer t;
+  t.start();
+  for (int i = 0; i < iters; ++i)
+    strided_read_kernel<<<dim3(ctas_per_pe, r.npes), 256>>>(r.cfg, off, set_off, nsets, rows, stride, sink);
+  t.stop();
+  if ((rc = last_launch("strided_read"))) return rc;
+  float ms = t.ms();
+  if (out_ms) *out_ms = ms;
+  return check_cuda(cudaDeviceSynchronize(), "strided_read");
 }
 
 int nvshmemx_op_wait_test(size_t flag_off, int value, long long timeout_ns, int *out_status) {

@@ -102,6 +102,7 @@ _SIGS = {
                                  c_int, _P(c_float)]),
     "nvshmemx_op_halo_offload": (c_int, [c_int, c_int, c_int, c_int, c_size_t, c_size_t, c_size_t, c_int,
                                          c_int, _P(c_float)]),
+    "nvshmemx_op_strided_read": (c_int, [c_size_t, c_size_t, c_int, c_size_t, c_size_t, c_int, c_int, _P(c_float)]),
     "nvshmemx_op_wait_test": (c_int, [c_size_t, c_int, c_longlong, _P(c_int)]),
     "nvshmemx_op_barrier_fault_test": (c_int, [c_int, c_longlong, _P(c_int)]),
     # nvshmemx_batch.h

@@ -137,6 +137,13 @@ class Shmem:
         check(fn(px, py, pz, n, block_off, ghost_off, sig_off, iters, ctas_per_pe, byref(ms)), "halo")
         return ms.value
 
+    def strided_read(self, off, set_off, nsets, rows, stride, ctas_per_pe, iters) -> float:
+        """nvshmemx_op_strided_read: device ms of `iters` scattered-read launches."""
+        ms = c_float(0)
+        check(lib.nvshmemx_op_strided_read(off, set_off, nsets, rows, stride, ctas_per_pe, iters, byref(ms)),
+              "strided_read")
+        return ms.value
+
     def wait_test(self, flag_off, value, timeout_ns) -> int:
         st = c_int(0)
         check(lib.nvshmemx_op_wait_test(flag_off, value, timeout_ns, byref(st)), "wait_test")

@@ -151,6 +151,17 @@ int nvshmemx_op_halo(int px, int py, int pz, int n, size_t block_off, size_t gho
 int nvshmemx_op_halo_offload(int px, int py, int pz, int n, size_t block_off, size_t ghost_off,
                              size_t sig_off, int iters, int ctas_per_pe, float *out_ms);
 
+/* ---- measurement: the halo's gather ceiling ------------------------------
+ * No counterpart in the reference.  Every PE reads nsets x rows 8-byte
+ * elements of its own slice, element i of set t at off + t * set_off +
+ * i * stride, with ctas_per_pe CTAs of 256 threads per PE and 8 loads in
+ * flight per thread, `iters` launches back to back; *out_ms their device
+ * time.  With the halo's x faces (rows = n*n, stride = 8n, sets at x = 0 and
+ * x = n-1) it is the time those faces need at best: the same scattered
+ * reads with nothing else to do. */
+int nvshmemx_op_strided_read(size_t off, size_t set_off, int nsets, size_t rows, size_t stride, int ctas_per_pe,
+                             int iters, float *out_ms);
+
 /* ---- failure detection ---------------------------------------------------
  * One thread of PE 0 waits (nvshmemx_int_wait_until_cmp EQ) on the int at
  * flag_off for `value` with the given deadline; returns the wait's status
