@@ -421,6 +421,47 @@ def run_c5_picker():
     return summary
 
 
+def run_c4_heldout_seeds(flush, seeds=(5, 6, 7, 8), reps=5):
+    """The tuned table's configuration (chosen on the seed-4 batch) against the
+    library default on C4 batches of other seeds: median graph step and exec
+    kernel time, L2 flushed before each run."""
+    from nvshmem_b200 import Shmem, default_batch_config, requests_bytes
+    from nvshmem_b200.traffic import c4_batch
+    tuned = load_tuned()
+    default = default_batch_config().as_dict()
+    out = {}
+    with Shmem(C4["npes"], C4["heap"]) as sh:
+        for pe in range(C4["npes"]):
+            sh.fill_random(pe, 0, C4["heap"], 44)
+        for seed in seeds:
+            reqs = c4_batch(**dict(C4, seed=seed))
+            alg = requests_bytes(reqs)
+            row = {}
+            with sh.batch(len(reqs), int(reqs["bytes"].sum()), 256) as b:
+                b.upload(reqs)
+                for name, cfg in (("tuned", tuned), ("default", default)):
+                    if not cfg:
+                        continue
+                    b.set_config(cfg)
+                    for _ in range(2):
+                        flush()
+                        b.execute(1)
+                    st, ex = [], []
+                    for _ in range(reps):
+                        flush()
+                        st.append(b.execute(1))
+                        flush()
+                        ex.append(b.execute_direct(1)[1])
+                    row[name] = {"step_us": round(1e3 * statistics.median(st), 1),
+                                 "exec_us": round(1e3 * statistics.median(ex), 1),
+                                 "GBps": round(alg / (statistics.median(st) / 1e3) / 1e9, 1)}
+            if "tuned" in row and "default" in row:
+                row["tuned_gain_pct"] = round(100 * (row["default"]["step_us"] / row["tuned"]["step_us"] - 1), 2)
+            out[f"seed{seed}"] = row
+        assert sh.status() == 0
+    return out
+
+
 def run_c4_picked(steps, flush):
     """The C4 batch through nvshmemx_batch_execute_picked: host requests
     grouped by size class, width and alignment, a variant picked per group by
@@ -579,6 +620,7 @@ def run_gpu(args, rank, world, local):
             out["c3_halo"] = run_c3_halo(peak)
             out["c5_picker_regret"] = run_c5_picker()
             out["c4_picked"] = run_c4_picked(max(3, args.steps // 4), flush)
+            out["c4_heldout_seeds"] = run_c4_heldout_seeds(flush)
     clocks = sampler.summary()
 
     value = world * alg * args.steps / t_batch / 1e9

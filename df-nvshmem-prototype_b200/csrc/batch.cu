@@ -1002,9 +1002,11 @@ int batch_sticky_status(nvshmemx_batch *b, int *status, int *bad_request) {
 
 extern "C" {
 
-// The autotuner's best on the 64-PE / 100,000-request workload: per-warp TMA
-// rings of 3 x 8 KiB, 8 warps per CTA, 16 KiB chunks, 2 chunks per claim,
-// register copy below 512 bytes.
+// Per-warp TMA rings of 3 x 8 KiB, 8 warps per CTA, 16 KiB chunks, 2 chunks
+// per claim, register copy below 512 bytes: one of the autotuner's leading
+// shapes on the 64-PE / 100,000-request workload (4th of 112, 1% behind the
+// table's best, 2 x 8 KiB rings with 4 warps per CTA; the first eight lie
+// within 1.5% of each other and their order changes from box to box).
 void nvshmemx_batch_default_config(nvshmemx_batch_config *c) {
   c->vec_bytes = 16;
   c->chunk_bytes = 16384;

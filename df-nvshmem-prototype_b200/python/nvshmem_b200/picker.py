@@ -53,8 +53,13 @@ def features(size, width, align, npes, pattern, inflight):
                     dtype=np.float32)
 
 
+MAX_INFLIGHT_LOG2 = 15           # groups of up to 32768 requests ...
+MAX_CLASS_BYTES = 128 << 20      # ... moving up to 128 MiB
+
+
 def sample_classes(seed: int, n: int, patterns=(0, 1, 2)):
-    """n random classes; sizes 4 B..4 MiB, in-flight 1..4096, total <= 32 MiB."""
+    """n random classes; sizes 4 B..4 MiB, in-flight 1..32768, total <= 128 MiB
+    (large groups are where one batch run beats per-request calls)."""
     st = Stream(seed)
     out = []
     while len(out) < n:
@@ -66,34 +71,32 @@ def sample_classes(seed: int, n: int, patterns=(0, 1, 2)):
             align = 8
         npes = [2, 8, 64][int(st.randint(1, 3)[0])]
         pattern = int(patterns[int(st.randint(1, len(patterns))[0])])
-        inflight = 1 << int(st.randint(1, 13)[0])             # 1..4096
+        inflight = 1 << int(st.randint(1, MAX_INFLIGHT_LOG2 + 1)[0])
         per_pe_cap = (ARENA_HEAP // 2 - (1 << 20)) * min(npes, inflight)
-        while inflight > 1 and (inflight * (size + 32) > (32 << 20) or inflight * (size + 32) > per_pe_cap):
+        while inflight > 1 and (inflight * (size + 32) > MAX_CLASS_BYTES or inflight * (size + 32) > per_pe_cap):
             inflight //= 2
         out.append(dict(size=size, width=width, align=align, npes=npes, pattern=pattern, inflight=inflight))
     return out
 
 
-def _dst_pe(pattern, i, src, npes, st):
+def _dst_pes(pattern, i, src, npes, st):
+    """Destination PE of request i (arrays) for each pattern."""
     if pattern == 0:
-        return 1 - src if npes >= 2 else 0
+        return 1 - src if npes >= 2 else np.zeros_like(src)
     if pattern == 1:
         return (src + 1 + (i // npes) % max(npes - 1, 1)) % npes
     if pattern == 2:
         px = 2 if npes == 8 else (4 if npes == 64 else 2)
         py = px if npes >= 8 else 1
-        x, y, z = src % px, (src // px) % py, src // (px * py)
         pz = max(npes // (px * py), 1)
+        x, y, z = src % px, (src // px) % py, src // (px * py)
         d = (i // npes) % 6
-        s = 1 if d & 1 else -1
-        if d < 2:
-            x = (x + s) % px
-        elif d < 4:
-            y = (y + s) % py
-        else:
-            z = (z + s) % pz
+        sgn = np.where(d & 1, 1, -1)
+        x = np.where(d < 2, (x + sgn) % px, x)
+        y = np.where((d >= 2) & (d < 4), (y + sgn) % py, y)
+        z = np.where(d >= 4, (z + sgn) % pz, z)
         return (x + px * (y + py * z)) % npes
-    return int(st.randint(1, npes)[0])
+    return st.randint(len(i), npes)
 
 
 def make_group(c: dict, seed: int) -> np.ndarray:
@@ -104,18 +107,31 @@ def make_group(c: dict, seed: int) -> np.ndarray:
     n, npes, size = c["inflight"], c["npes"], c["size"]
     skew = {16: 0, 8: 8, 4: 4}[c["align"]]
     half = ARENA_HEAP // 2
+    i = np.arange(n, dtype=np.int64)
+    if c["pattern"] in (1, 2):
+        src = i % npes
+    elif c["pattern"] == 0:
+        src = (i % 2) * (1 % npes)
+    else:
+        src = st.randint(n, npes)
+    dst = _dst_pes(c["pattern"], i, src, npes, st)
+    # destinations: consecutive slots per destination PE in request order
+    occ = (size + skew + 31) // 16 * 16
+    order = np.argsort(dst, kind="stable")
+    rank = np.empty(n, dtype=np.int64)
+    sd = dst[order]
+    starts = np.r_[0, np.nonzero(np.diff(sd))[0] + 1]
+    pos = np.arange(n) - np.repeat(starts, np.diff(np.r_[starts, n]))
+    rank[order] = pos
+    span = max((half - size - 64) // 16, 1)
     r = np.zeros(n, dtype=REQUEST_DTYPE)
-    cursor = {}
-    for i in range(n):
-        src = i % npes if c["pattern"] in (1, 2) else (0 if c["pattern"] == 0 else int(st.randint(1, npes)[0]))
-        if c["pattern"] == 0 and i % 2:
-            src = 1 % npes
-        dst = _dst_pe(c["pattern"], i, src, npes, st)
-        slot = cursor.get(dst, half)
-        cursor[dst] = slot + (size + skew + 31) // 16 * 16
-        span = max((half - size - 64) // 16, 1)
-        r[i] = (int(st.randint(1, span)[0]) * 16, slot + skew, size, src, dst, i % 2,
-                2 if c["width"] == 8 else 1, 0, 0)
+    r["src_off"] = st.randint(n, span) * 16
+    r["dst_off"] = half + rank * occ + skew
+    r["bytes"] = size
+    r["src_pe"] = src
+    r["dst_pe"] = dst
+    r["op"] = i % 2
+    r["dtype"] = 2 if c["width"] == 8 else 1
     return r
 
 
@@ -127,7 +143,7 @@ def measure(classes, seed0: int, reps: int = 3, flush_bytes: int = 256 << 20, lo
     with Shmem(ARENA_PES, ARENA_HEAP) as sh:
         for pe in range(ARENA_PES):
             sh.fill_random(pe, 0, ARENA_HEAP, 7)
-        with sh.batch(4096, 256 << 20, 1024) as b:
+        with sh.batch(1 << MAX_INFLIGHT_LOG2, 2 * MAX_CLASS_BYTES, 1024) as b:
             for ci, c in enumerate(classes):
                 g = make_group(c, seed0 + ci)
                 # halve the group until every destination fits its PE's heap

@@ -55,8 +55,9 @@ typedef struct nvshmemx_batch_config {
   int stream_planners; /* planning warps per CTA in stream mode: 1..4        */
 } nvshmemx_batch_config;
 
-/* Defaults for B200: the best configuration the autotuner measured on the
- * 64-PE, 100,000-request workload (see tuned/batch_c4.json). */
+/* Defaults for B200: one of the leading configurations the autotuner
+ * measured on the 64-PE, 100,000-request workload (tuned/batch_c4.json holds
+ * the measured table and its best). */
 void nvshmemx_batch_default_config(nvshmemx_batch_config *cfg);
 
 typedef struct nvshmemx_batch nvshmemx_batch;
