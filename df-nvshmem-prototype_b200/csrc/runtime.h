@@ -32,7 +32,6 @@ struct Runtime {
   int *d_status = nullptr;
   unsigned long long *d_coll_bar = nullptr;
   unsigned long long *d_pe_bar = nullptr;
-  unsigned long long *d_offload_bar = nullptr;
   size_t bar_reset_bytes = 0;  // bytes from d_coll_bar to reset before a collective launch
   long long wait_timeout_ns = 5000000000LL;
   int error_mode = NVSHMEMX_ERRORS_EXIT;
