@@ -509,7 +509,7 @@ __device__ __forceinline__ void halo_xrow_put(const Cfg &c, double *dst_sym, con
     for (int u = 0; u < 8; ++u) {
       const int k = k0 + u * 32 + (int)lane;
       if (k < n)
-        asm volatile("ld.global.nc.L1::no_allocate.b64 %0, [%1];" : "=l"(v[u]) : "l"(s + k * stride));
+        asm volatile("ld.global.nc.L1::no_allocate.L2::64B.b64 %0, [%1];" : "=l"(v[u]) : "l"(s + k * stride));
     }
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
@@ -531,7 +531,10 @@ __global__ void __launch_bounds__(256, 4) halo_kernel(Cfg c, int px, int py, int
   int *my_sig = (int *)slice_ptr(c, pe, sig_off);
   for (int it = 0; it < iters; ++it) {
     for (long long u = gw; u < 6ll * n; u += nw) {
-      const int d = (int)(u / n), j = (int)(u % n);
+      // units 0 .. 2n-1 pair the two x faces row by row (unit 2j reads
+      // element x = 0 and unit 2j+1 element x = n-1 of the same 2 KiB rows,
+      // on neighbouring warps at about the same time), then the y and z faces
+      const int d = u < 2ll * n ? (int)(u & 1) : (int)(u / n), j = u < 2ll * n ? (int)(u >> 1) : (int)(u % n);
       const int nb = halo_nbr(pe, d, px, py, pz);
       double *dst = (double *)(c.arena + ghost_off + (unsigned long long)(d ^ 1) * face_bytes +
                                (unsigned long long)j * n * 8ull);
@@ -567,8 +570,10 @@ __global__ void __launch_bounds__(256, 4) halo_kernel(Cfg c, int px, int py, int
 // What the halo's x faces cost at best: every PE reads nsets x rows 8-byte
 // elements, element i of set t at slice offset off + t * set_off +
 // i * stride, with ctas_per_pe CTAs per PE and 8 loads in flight per lane
-// (the access pattern of halo_xrow_put without its stores), and adds them
-// into one word per warp so that nothing is optimised away.
+// (the access pattern of halo_xrow_put without its stores; consecutive
+// threads take the sets of one row in turn, as the halo pairs its two x
+// faces), and adds them into one word per warp so that nothing is optimised
+// away.
 __global__ void __launch_bounds__(256) strided_read_kernel(Cfg c, unsigned long long off, unsigned long long set_off,
                                                            int nsets, unsigned long long rows,
                                                            unsigned long long stride, unsigned long long *sink) {
@@ -585,9 +590,9 @@ __global__ void __launch_bounds__(256) strided_read_kernel(Cfg c, unsigned long 
       const unsigned long long i = i0 + (unsigned long long)u * nthr;
       v[u] = 0;
       if (i < total) {
-        const unsigned long long set = i / rows, row = i - set * rows;
+        const unsigned long long set = i % (unsigned long long)nsets, row = i / (unsigned long long)nsets;
         const char *p = base + set * set_off + row * stride;
-        asm volatile("ld.global.nc.L1::no_allocate.b64 %0, [%1];" : "=l"(v[u]) : "l"(p));
+        asm volatile("ld.global.nc.L1::no_allocate.L2::64B.b64 %0, [%1];" : "=l"(v[u]) : "l"(p));
       }
     }
 #pragma unroll
