@@ -163,7 +163,7 @@ def test_alltoall_every_c2_size(shmem_factory):
 
 
 @pytest.mark.parametrize("offload", [False, True], ids=["persistent", "offload_barrier"])
-@pytest.mark.parametrize("n", [8, 32])
+@pytest.mark.parametrize("n", [8, 32, 40])
 def test_halo_bit_exact(shmem_factory, n, offload):
     npes = 8
     block = n * n * n * 8

@@ -52,6 +52,29 @@ def test_trace_ring_records_and_csv(shmem_factory, tmp_path):
     sh.trace_disable()
 
 
+def test_offload_barrier_and_halo_trace_records(shmem_factory):
+    """Every nvshmem_barrier_all_offload leaves one BARRIER record per PE, and
+    the halo records one PUT per face row (x rows as put_double)."""
+    npes, n = 8, 32
+    block, ghosts = n ** 3 * 8, 6 * n * n * 8
+    sh = shmem_factory(npes, block + ghosts + 4096)
+    sh.trace_enable(1 << 14)
+    for _ in range(3):
+        lib.nvshmem_barrier_all_offload()
+    sh.sync()
+    for pe in range(npes):
+        rec, dropped = sh.trace_read(pe)
+        assert dropped == 0 and (rec["op"] == 8).sum() == 3 and np.all(rec["pe"] == pe)
+    sh.trace_enable(1 << 14)  # a fresh ring
+    sh.halo(2, 2, 2, n, 0, block, block + ghosts, 1, 2)
+    assert sh.status() == 0
+    for pe in range(npes):
+        rec, _ = sh.trace_read(pe)
+        assert ((rec["op"] == 2) & (rec["bytes"] == n * 8)).sum() == 2 * n  # x-face rows
+        assert ((rec["op"] == 0) & (rec["bytes"] == n * 8)).sum() == 4 * n  # y and z rows
+    sh.trace_disable()
+
+
 CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p)
 
 
