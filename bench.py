@@ -485,13 +485,16 @@ def run_c4_picked(steps, flush):
             b.upload(reqs)
             b.execute(1)
             want = [sh.checksum(pe, 0, C4["heap"]) for pe in range(C4["npes"])]
-            ms = []
+            ms, run_ms = [], []
+            hb = b.host_buffer()
+            hb[:len(reqs)] = reqs
             for i in range(steps + 1):
                 flush()
-                st, t, groups = b.execute_picked(pk, reqs, PATTERN_RANDOM)
+                st, t, tr, groups = b.execute_picked(pk, hb[:len(reqs)], PATTERN_RANDOM)
                 assert st == 0, f"picked execution status {st}"
                 if i:
                     ms.append(t)
+                    run_ms.append(tr)
             got = [sh.checksum(pe, 0, C4["heap"]) for pe in range(C4["npes"])]
             assert got == want, "picked execution differs from the batch engine"
         assert sh.status() == 0
@@ -500,12 +503,14 @@ def run_c4_picked(steps, flush):
     for g in groups:
         k = picker.VARIANT_NAMES[int(g["variant"])]
         per_variant[k] = per_variant.get(k, 0) + int(g["count"])
-    med = statistics.median(ms)
-    return {"GBps": round(alg / (med / 1e3) / 1e9, 1), "ms": round(med, 4), "groups": int(len(groups)),
+    med, run = statistics.median(ms), statistics.median(run_ms)
+    return {"GBps": round(alg / (med / 1e3) / 1e9, 1), "ms": round(med, 4),
+            "run_GBps": round(alg / (run / 1e3) / 1e9, 1), "run_ms": round(run, 4), "groups": int(len(groups)),
             "decided_by": {"network": int((groups["source"] == 0).sum()), "table": int((groups["source"] == 1).sum()),
                            "fixed": int((groups["source"] == 2).sum())},
             "requests_per_variant": per_variant,
-            "timing": "device time from the host-to-device request copy to the end of the last run"}
+            "timing": ("GBps / ms: device time from the start of the host-to-device copy of the 32-byte requests "
+                       "(from pinned memory) to the end of the last run; run_GBps / run_ms: after the copy")}
 
 
 def cpu_latency():

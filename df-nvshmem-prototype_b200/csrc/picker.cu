@@ -40,6 +40,7 @@ struct nvshmemx_picker {
   // batch runs and each other), and the events that fork and join them
   cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t ev_copied = nullptr, ev_done[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev_t[3] = {nullptr, nullptr, nullptr};  // timing: start, requests copied, end
   int nt = 0;
   std::vector<float> tx, tt;  // nt x kNin features, nt x kNv times (ms)
   float mean[kNin], sd[kNin], lo[kNin], hi[kNin];
@@ -109,6 +110,7 @@ int nvshmemx_picker_create(nvshmemx_mlp *net, const float *table_x, const float 
   }
   int rc = nvshmemx_mlp_set_normalization(net, p->mean, p->sd);
   if (!rc) rc = check_cuda(cudaEventCreateWithFlags(&p->ev_copied, cudaEventDisableTiming), "cudaEventCreate");
+  for (int k = 0; k < 3 && !rc; ++k) rc = check_cuda(cudaEventCreate(&p->ev_t[k]), "cudaEventCreate");
   for (int m = 0; m < 4 && !rc; ++m) {
     rc = check_cuda(cudaStreamCreateWithFlags(&p->aux[m], cudaStreamNonBlocking), "cudaStreamCreate");
     if (!rc) rc = check_cuda(cudaEventCreateWithFlags(&p->ev_done[m], cudaEventDisableTiming), "cudaEventCreate");
@@ -131,6 +133,8 @@ int nvshmemx_picker_destroy(nvshmemx_picker *p) {
     if (p->ev_done[m]) cudaEventDestroy(p->ev_done[m]);
   }
   if (p->ev_copied) cudaEventDestroy(p->ev_copied);
+  for (int k = 0; k < 3; ++k)
+    if (p->ev_t[k]) cudaEventDestroy(p->ev_t[k]);
   delete p;
   return 0;
 }
@@ -198,7 +202,7 @@ struct Group {
 
 extern "C" int nvshmemx_batch_execute_picked(nvshmemx_batch *b, nvshmemx_picker *p, const nvshmemx_request *reqs,
                                              int n, int pattern, nvshmemx_picked_group *groups, int max_groups,
-                                             int *ngroups, int *out_status, float *out_ms) {
+                                             int *ngroups, int *out_status, float *out_ms, float *out_run_ms) {
   if (!is_started()) return fail(NVSHMEMX_ERR_STATE, "batch_execute_picked before nvstart_pes");
   if (!b || !p || n < 0 || (n && !reqs) || n > batch_capacity(b) || pattern < 0 || pattern > 3 ||
       (max_groups > 0 && !groups))
@@ -206,6 +210,7 @@ extern "C" int nvshmemx_batch_execute_picked(nvshmemx_batch *b, nvshmemx_picker 
   if (ngroups) *ngroups = 0;
   if (out_status) *out_status = 0;
   if (out_ms) *out_ms = 0.f;
+  if (out_run_ms) *out_run_ms = 0.f;
   if (n == 0) return 0;
   const Runtime &r = rt();
   for (int i = 0; i < n; ++i) {
@@ -271,13 +276,26 @@ extern "C" int nvshmemx_batch_execute_picked(nvshmemx_batch *b, nvshmemx_picker 
   }
   // ---- grouped order: groups sorted by variant, so each variant is one run
   std::stable_sort(gs.begin(), gs.end(), [](const Group &a, const Group &c) { return a.variant < c.variant; });
-  std::vector<nvshmemx_request> perm;
-  perm.reserve((size_t)n);
-  std::vector<int> first(gs.size());
-  for (size_t k = 0; k < gs.size(); ++k) {
-    first[k] = (int)perm.size();
-    for (int i : gs[k].idx) perm.push_back(reqs[i]);
+  // The grouped order is written into the batch's pinned host buffer, so the
+  // copy to the device runs at the host link's speed (from pageable memory
+  // the driver would stage it at a fraction of that); when the caller's
+  // requests already sit in that buffer, they are gathered through a
+  // temporary array first.
+  nvshmemx_request *pinned = nvshmemx_batch_host_buffer(b);
+  const bool aliased = reqs < pinned + batch_capacity(b) && pinned < reqs + n;
+  std::vector<nvshmemx_request> tmp;
+  nvshmemx_request *perm = pinned;
+  if (aliased) {
+    tmp.resize((size_t)n);
+    perm = tmp.data();
   }
+  std::vector<int> first(gs.size());
+  size_t at = 0;
+  for (size_t k = 0; k < gs.size(); ++k) {
+    first[k] = (int)at;
+    for (int i : gs[k].idx) perm[at++] = reqs[i];
+  }
+  if (aliased) memcpy(pinned, tmp.data(), (size_t)n * sizeof(nvshmemx_request));
   if (ngroups) *ngroups = (int)gs.size();
   for (size_t k = 0; k < gs.size() && (int)k < max_groups; ++k) {
     groups[k].first = first[k];
@@ -289,15 +307,13 @@ extern "C" int nvshmemx_batch_execute_picked(nvshmemx_batch *b, nvshmemx_picker 
   // ---- run: one request copy, then one launch or batch run per variant
   cudaStream_t st = batch_stream(b);
   nvshmemx_request *d = batch_device_requests(b);
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  int rc = check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
-  if (!rc) rc = check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
-  if (!rc) rc = check_cuda(cudaEventRecord(e0, st), "cudaEventRecord");
+  int rc = check_cuda(cudaEventRecord(p->ev_t[0], st), "cudaEventRecord");
   if (!rc)
-    rc = check_cuda(cudaMemcpyAsync(d, perm.data(), (size_t)n * sizeof(nvshmemx_request), cudaMemcpyHostToDevice, st),
+    rc = check_cuda(cudaMemcpyAsync(d, pinned, (size_t)n * sizeof(nvshmemx_request), cudaMemcpyHostToDevice, st),
                     "cudaMemcpyAsync(requests)");
   if (!rc) rc = batch_clear_sticky(b);
   if (!rc) rc = check_cuda(cudaEventRecord(p->ev_copied, st), "cudaEventRecord");
+  if (!rc) rc = check_cuda(cudaEventRecord(p->ev_t[1], st), "cudaEventRecord");
   nvshmemx_batch_config own;
   nvshmemx_batch_get_config(b, &own);
   bool used[4] = {false, false, false, false};
@@ -328,16 +344,16 @@ extern "C" int nvshmemx_batch_execute_picked(nvshmemx_batch *b, nvshmemx_picker 
       const int wr = check_cuda(cudaStreamWaitEvent(st, p->ev_done[m], 0), "cudaStreamWaitEvent");
       if (!rc) rc = wr;
     }
-  if (!rc) rc = check_cuda(cudaEventRecord(e1, st), "cudaEventRecord");
+  if (!rc) rc = check_cuda(cudaEventRecord(p->ev_t[2], st), "cudaEventRecord");
   if (!rc) rc = check_cuda(cudaStreamSynchronize(st), "batch_execute_picked");
-  float ms = 0;
-  if (!rc) cudaEventElapsedTime(&ms, e0, e1);
-  if (e0) cudaEventDestroy(e0);
-  if (e1) cudaEventDestroy(e1);
   if (rc) return rc;
+  float ms = 0, run_ms = 0;
+  cudaEventElapsedTime(&ms, p->ev_t[0], p->ev_t[2]);
+  cudaEventElapsedTime(&run_ms, p->ev_t[1], p->ev_t[2]);
   int s0 = 0, bad = 0;
   if ((rc = batch_sticky_status(b, &s0, &bad))) return rc;
   if (out_status) *out_status = s0;
   if (out_ms) *out_ms = ms;
+  if (out_run_ms) *out_run_ms = run_ms;
   return 0;
 }

@@ -140,7 +140,7 @@ _SIGS = {
     "nvshmemx_picker_pick": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     "nvshmemx_picker_table_pick": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
     "nvshmemx_batch_execute_picked": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_int,
-                                              _P(c_int), _P(c_int), _P(c_float)]),
+                                              _P(c_int), _P(c_int), _P(c_float), _P(c_float)]),
     # nvshmemx_tune.h
     "nvshmemx_tune_candidates": (c_int, [_P(BatchConfig), c_int, c_int]),
     "nvshmemx_tune_batch": (c_int, [c_void_p, _P(BatchConfig), c_int, c_int, c_size_t, _P(TuneResult),

@@ -271,14 +271,15 @@ class Batch:
         return ms.value
 
     def execute_picked(self, picker, reqs: np.ndarray, pattern: int = L.PATTERN_RANDOM, max_groups: int = 256):
-        """nvshmemx_batch_execute_picked: (status, device ms, groups) for the
-        host requests `reqs` run group by group with the picker's variants."""
+        """nvshmemx_batch_execute_picked: (status, device ms with the request
+        copy, device ms after it, groups) for the host requests `reqs` run
+        group by group with the picker's variants."""
         r = np.ascontiguousarray(reqs, dtype=L.REQUEST_DTYPE)
         groups = np.zeros(max_groups, L.PICKED_GROUP_DTYPE)
-        ng, st, ms = c_int(0), c_int(0), c_float(0)
+        ng, st, ms, run = c_int(0), c_int(0), c_float(0), c_float(0)
         check(lib.nvshmemx_batch_execute_picked(self.h, picker.h, ptr(r), len(r), pattern, ptr(groups), max_groups,
-                                                byref(ng), byref(st), byref(ms)), "batch_execute_picked")
-        return st.value, ms.value, groups[:min(ng.value, max_groups)]
+                                                byref(ng), byref(st), byref(ms), byref(run)), "batch_execute_picked")
+        return st.value, ms.value, run.value, groups[:min(ng.value, max_groups)]
 
     def stats(self):
         ch = c_ulonglong(0)

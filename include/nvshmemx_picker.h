@@ -119,11 +119,14 @@ typedef struct nvshmemx_picked_group {
  * request array (so n <= its max_requests) in grouped order.  groups
  * (room for max_groups entries, may be NULL) receives the groups, *ngroups
  * their count; *out_status the first execution error (0: every request
- * done); *out_ms the device time from the request copy to the end of the
- * last run. */
+ * done); *out_ms the device time from the start of the request copy to the
+ * end of the last run, *out_run_ms the part after the copy (both may be
+ * NULL).  The requests reach the device through the batch's pinned host
+ * buffer (nvshmemx_batch_host_buffer), which the call overwrites; passing
+ * that buffer itself as reqs is allowed. */
 int nvshmemx_batch_execute_picked(nvshmemx_batch *b, nvshmemx_picker *p, const nvshmemx_request *reqs, int n,
                                   int pattern, nvshmemx_picked_group *groups, int max_groups, int *ngroups,
-                                  int *out_status, float *out_ms);
+                                  int *out_status, float *out_ms, float *out_run_ms);
 
 /* Execution of variant v (0..11) on b's uploaded requests, with L2 flushed
  * before each of `reps` runs; *out_ms = median device time. */

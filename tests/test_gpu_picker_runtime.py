@@ -66,10 +66,12 @@ def test_network_inside_the_range_table_outside():
 
 def _execute(b, h, reqs, pattern=3):
     groups = np.zeros(64, PICKED_GROUP_DTYPE)
-    ng, st, ms = c_int(), c_int(), c_float()
+    ng, st, ms, run = c_int(), c_int(), c_float(), c_float()
     r = np.ascontiguousarray(reqs)
     rc = L.lib.nvshmemx_batch_execute_picked(b.h, h, r.ctypes.data, len(r), pattern, groups.ctypes.data, len(groups),
-                                             byref(ng), byref(st), byref(ms))
+                                             byref(ng), byref(st), byref(ms), byref(run))
+    if rc == 0:
+        assert 0 < run.value <= ms.value
     return rc, groups[:ng.value], st.value, ms.value
 
 
@@ -134,6 +136,31 @@ def test_execute_picked_with_the_trained_picker_on_c4_traffic(shmem_factory):
     om.apply_requests(reqs)
     assert first_diff(heap_images(sh, npes, heap), om.heap) is None
     pk.close()
+
+
+def test_execute_picked_from_the_batch_pinned_buffer(shmem_factory):
+    """The requests may already sit in the batch's pinned host buffer, which
+    the call also uses to stage the grouped order."""
+    npes, heap = 8, 2 << 20
+    sh = shmem_factory(npes, heap)
+    om = Model(npes, heap)
+    for pe in range(npes):
+        sh.fill_random(pe, 0, heap, 13)
+        om.fill_random(pe, 0, heap, 13)
+    reqs = random_requests(77, 500, npes, heap, max_bytes=30000)
+    net = P.MLP(seed=2)
+    h, keep = _picker(net, np.full((1, 6), 100.0, np.float32), np.ones((1, NV), np.float32))
+    try:
+        with sh.batch(len(reqs), int(reqs["bytes"].sum()) + 8 * len(reqs), 256) as b:
+            buf = b.host_buffer()
+            buf[:len(reqs)] = reqs
+            rc, groups, st, _ = _execute(b, h, buf[:len(reqs)])
+            assert rc == 0 and st == 0 and groups["count"].sum() == len(reqs)
+        assert sh.status() == 0
+        om.apply_requests(reqs)
+        assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+    finally:
+        L.lib.nvshmemx_picker_destroy(h)
 
 
 def test_execute_picked_rejects_before_running(shmem_factory):
