@@ -211,6 +211,44 @@ def test_submit_compact(shmem_factory, cfg, n):
     sh.status()
 
 
+@pytest.mark.parametrize("where", ["pinned", "pageable"])
+def test_submit_compact_first_piece_error_and_host_memory(shmem_factory, where):
+    """Two pieces of compact requests, from the batch's pinned buffer (the
+    first piece planned straight from host memory) or from ordinary host
+    memory (copied first): a valid batch matches the oracle, and an invalid
+    request in the first piece stops everything."""
+    from nvshmem_b200 import ERR_INVALID, to_compact
+    npes, heap, n = 16, 32 << 20, 30000
+    reqs = c4_batch(seed=50, n=n, npes=npes, heap=heap, hi=16 << 10)
+    sh, om = setup(shmem_factory, npes, heap)
+    with sh.batch(len(reqs), int(reqs["bytes"].sum()), 256) as b:
+        comp = to_compact(reqs)
+        if where == "pinned":
+            buf = b.host_buffer_compact()
+            buf[:n] = comp
+            src = buf[:n]
+        else:
+            src = comp.copy()
+        st, ms = b.submit_compact(src, n)
+        assert st == 0 and ms > 0
+        om.apply_requests(reqs)
+        assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+        for pe in range(npes):
+            sh.fill_random(pe, 0, heap, 9)
+        before = heap_images(sh, npes, heap)
+        bad = comp.copy()
+        bad[123]["meta"] |= 1 << 31
+        if where == "pinned":
+            buf[:n] = bad
+            src = buf[:n]
+        else:
+            src = bad
+        st, _ = b.submit_compact(src, n)
+        assert st == ERR_INVALID
+        assert np.array_equal(heap_images(sh, npes, heap), before)
+    sh.status()
+
+
 def test_submit_compact_needs_a_graph_configuration(shmem_factory):
     from nvshmem_b200 import ShmemError, to_compact
     sh, _ = setup(shmem_factory, 4, 1 << 20)
