@@ -316,6 +316,7 @@ extern "C" int nvshmemx_batch_execute_picked(nvshmemx_batch *b, nvshmemx_picker 
   if (!rc) rc = check_cuda(cudaEventRecord(p->ev_t[1], st), "cudaEventRecord");
   nvshmemx_batch_config own;
   nvshmemx_batch_get_config(b, &own);
+  if (own.stream) nvshmemx_batch_default_config(&own);  // runs here are plan-then-exec
   bool used[4] = {false, false, false, false};
   for (size_t k = 0; k < gs.size() && !rc;) {
     size_t e = k;
@@ -335,6 +336,7 @@ extern "C" int nvshmemx_batch_execute_picked(nvshmemx_batch *b, nvshmemx_picker 
       // a shape whose chunk is below the batch's smallest chunk would not
       // fit its chunk table: run it with the batch's own configuration
       if (c.chunk_bytes < batch_min_chunk(b)) c = own;
+      if (c.chunk_bytes < batch_min_chunk(b)) c.chunk_bytes = (batch_min_chunk(b) + 255) / 256 * 256;
       rc = batch_enqueue_range(b, first[k], count, c);
     }
     k = e;
