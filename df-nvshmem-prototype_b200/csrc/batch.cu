@@ -883,6 +883,10 @@ static int enqueue_piece(nvshmemx_batch *b, bool with_events, const void *src, i
   int per_sm = 0;
   if (tfn) {
     cudaFuncSetAttribute((const void *)tfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the rings are all the shared memory a CTA uses: ask for the largest
+    // shared-memory carveout, so the CTAs the occupancy query counts on fit
+    cudaFuncSetAttribute((const void *)tfn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)tfn, k.threads, smem);
   } else {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, k.threads, 0);
@@ -1431,6 +1435,10 @@ extern "C" int nvshmemx_batch_execute_noalloc(const nvshmemx_request *d_reqs, in
   const size_t smem = tfn ? tma_smem_bytes(k) : 0;
   if (tfn) {
     cudaFuncSetAttribute((const void *)tfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the rings are all the shared memory a CTA uses: ask for the largest
+    // shared-memory carveout, so the CTAs the occupancy query counts on fit
+    cudaFuncSetAttribute((const void *)tfn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)tfn, k.threads, smem);
   } else {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, k.threads, 0);
