@@ -490,6 +490,52 @@ int nvshmemx_init_process(int pe, int npes, size_t heap_bytes_per_pe, const char
   return init_impl(npes, heap_bytes_per_pe, pe, rendezvous_dir);
 }
 
+// The application's launcher (MPI or any other) provides rank, size and an
+// allgather: rank 0's rendezvous directory name goes to every rank, every
+// rank starts process mode in it, a second allgather tells every rank that
+// all started, and rank 0 then empties and removes the directory (the
+// sockets and the barrier file are only opened during start-up; the barrier
+// stays mapped).
+int nvshmemx_init_bootstrap(const nvshmemx_bootstrap *bs, size_t heap_bytes_per_pe) {
+  constexpr size_t kName = 256;
+  if (!bs || !bs->allgather || bs->size < 1 || bs->rank < 0 || bs->rank >= bs->size)
+    return fail(NVSHMEMX_ERR_INVALID, "nvshmemx_init_bootstrap: bad bootstrap description");
+  char mine[kName];
+  memset(mine, 0, sizeof mine);
+  if (bs->rank == 0) {
+    const char *t = getenv("TMPDIR");
+    std::string tmpl = std::string(t && *t ? t : "/tmp") + "/nvshm-XXXXXX";
+    std::vector<char> name(tmpl.begin(), tmpl.end());
+    name.push_back('\0');
+    if (name.size() < kName && mkdtemp(name.data())) memcpy(mine, name.data(), name.size());
+    // on failure the empty name tells every rank to stop
+  }
+  std::vector<char> all((size_t)bs->size * kName);
+  if (bs->allgather(mine, all.data(), kName, bs->ctx) != 0)
+    return fail(NVSHMEMX_ERR_STATE, "nvshmemx_init_bootstrap: the allgather callback failed");
+  const std::string dir(all.data(), strnlen(all.data(), kName - 1));
+  if (dir.empty()) return fail(NVSHMEMX_ERR_STATE, "nvshmemx_init_bootstrap: rank 0 could not make a rendezvous directory");
+  int rc = nvshmemx_init_process(bs->rank, bs->size, heap_bytes_per_pe, dir.c_str());
+  const int started = rc == 0 ? 1 : 0;
+  std::vector<int> all_started((size_t)bs->size, 0);
+  const int grc = bs->allgather(&started, all_started.data(), sizeof(int), bs->ctx);
+  if (bs->rank == 0) {
+    for (int p = 0; p < bs->size; ++p) unlink((dir + "/pe" + std::to_string(p) + ".sock").c_str());
+    unlink((dir + "/barrier").c_str());
+    rmdir(dir.c_str());
+  }
+  bool everyone = grc == 0;
+  for (int s : all_started) everyone = everyone && s == 1;
+  if (!everyone) {
+    if (rc == 0) {
+      nvshmemx_finalize();
+      rc = fail(NVSHMEMX_ERR_STATE, "nvshmemx_init_bootstrap: another rank did not start");
+    }
+    return rc;
+  }
+  return 0;
+}
+
 int nvshmemx_finalize(void) {
   Runtime &r = rt();
   std::lock_guard<std::recursive_mutex> lk(r.mu);

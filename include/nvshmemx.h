@@ -94,6 +94,29 @@ int nvshmemx_init_attr(int npes, size_t heap_bytes_per_pe);
  * NVSHMEM_RENDEZVOUS are set (python -m nvshmem_b200.launch sets them);
  * NVSHMEM_DEVICE, when set, selects this process's device first. */
 int nvshmemx_init_process(int pe, int npes, size_t heap_bytes_per_pe, const char *rendezvous_dir);
+
+/* Process-per-PE mode started by the application's own launcher: the
+ * prototype bootstraps through MPI inside nvstart_pes (MPI_Comm_rank/size,
+ * MPI_Allgather of its IPC handles, MPI_Barrier; nvshmem.cu:480-561).  Here
+ * the caller hands over its rank, size and an allgather callback (for an MPI
+ * program, a wrapper of MPI_Allgather with MPI_BYTE on its communicator), and
+ * this process becomes PE `rank` of `size` as with nvshmemx_init_process.
+ * The callback is called with identical `len` by every rank and must fill
+ * out[size * len] with every rank's `len` bytes in rank order, returning 0 on
+ * success.  Rank 0 makes a private rendezvous directory under $TMPDIR (or
+ * /tmp) and shares its name through the callback; once every process has
+ * mapped every slice (a second allgather of each rank's start status), rank 0
+ * removes the directory's entries, which nothing uses after start-up.  All
+ * processes must be on one node (slices are exchanged as POSIX file
+ * descriptors).  Returns 0 when every rank started; otherwise no rank is
+ * left started. */
+typedef struct nvshmemx_bootstrap {
+  int rank;
+  int size;
+  int (*allgather)(const void *in, void *out, size_t len, void *ctx);
+  void *ctx;
+} nvshmemx_bootstrap;
+int nvshmemx_init_bootstrap(const nvshmemx_bootstrap *bs, size_t heap_bytes_per_pe);
 /* nvstop_pes with a status code. */
 int nvshmemx_finalize(void);
 int nvshmemx_is_started(void);

@@ -20,10 +20,10 @@ pytestmark = pytest.mark.gpu
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def build(tmp_path):
-    exe = tmp_path / "proc_pes"
+def build(tmp_path, name="proc_pes"):
+    exe = tmp_path / name
     r = subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-rdc=true",
-                        "-I", os.path.join(REPO, "include"), os.path.join(REPO, "tests", "native", "proc_pes.cu"),
+                        "-I", os.path.join(REPO, "include"), os.path.join(REPO, "tests", "native", name + ".cu"),
                         "-o", str(exe), "-L", os.path.join(REPO, "df-nvshmem-prototype_b200", "lib"), "-lnvshmem",
                         "-L/usr/local/cuda/lib64/stubs", "-lcuda"], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
@@ -40,16 +40,9 @@ def visible_devices():
     return torch.cuda.device_count()
 
 
-@pytest.mark.parametrize("npes,spread", [(2, False), (4, False), (4, True)])
-def test_processes_exchange_blocks(tmp_path, npes, spread):
-    """spread: the launcher's --devices over every visible GPU (contiguous
-    blocks of PEs per device; on a one-GPU box every PE names device 0)."""
-    exe = build(tmp_path)
-    heap = 4 << 20
-    codes = launch([exe, "exchange", str(tmp_path)], npes, heap=heap, timeout=240,
-                   env=dict(os.environ, NVSHMEM_HOST_BARRIER_TIMEOUT_S="60"),
-                   devices=visible_devices() if spread else None)
-    assert codes == [0] * npes, codes
+def check_exchange(tmp_path, npes, heap):
+    """The heaps the exchange of proc_pes.cu / boot_pes.cu wrote, against the
+    oracle: PE p's block in PE p+1's slot p and in PE p+1's `got` area."""
     rows = [list(map(int, (tmp_path / f"pe{pe}.txt").read_text().split())) for pe in range(npes)]
     assert sorted(r[0] for r in rows) == list(range(npes))
     _, send, recv, got, n = rows[0]
@@ -65,6 +58,19 @@ def test_processes_exchange_blocks(tmp_path, npes, spread):
     om.apply_requests(requests(ring))
     om.apply_requests(requests(pull))
     assert first_diff(images, om.heap) is None
+
+
+@pytest.mark.parametrize("npes,spread", [(2, False), (4, False), (4, True)])
+def test_processes_exchange_blocks(tmp_path, npes, spread):
+    """spread: the launcher's --devices over every visible GPU (contiguous
+    blocks of PEs per device; on a one-GPU box every PE names device 0)."""
+    exe = build(tmp_path)
+    heap = 4 << 20
+    codes = launch([exe, "exchange", str(tmp_path)], npes, heap=heap, timeout=240,
+                   env=dict(os.environ, NVSHMEM_HOST_BARRIER_TIMEOUT_S="60"),
+                   devices=visible_devices() if spread else None)
+    assert codes == [0] * npes, codes
+    check_exchange(tmp_path, npes, heap)
 
 
 def test_departed_process_fails_the_barrier(tmp_path):
@@ -104,3 +110,25 @@ def test_process_start_failures_leave_the_library_usable(tmp_path):
     rc1, rc2, rc3, dt = r.stdout.split()
     assert int(rc1) != 0 and int(rc2) != 0 and int(rc3) == 0
     assert 1.5 <= float(dt) <= 30  # the missing peer is given up on after the timeout
+
+
+@pytest.mark.parametrize("npes", [2, 4])
+def test_bootstrap_from_the_applications_own_launcher(tmp_path, npes):
+    """nvshmemx_init_bootstrap: the application forks its PE processes and
+    provides the allgather (the stand-in for MPI_Allgather), as an MPI program
+    would; the same exchange then matches the oracle, and the rendezvous
+    directory rank 0 made is gone afterwards."""
+    import signal
+    exe = build(tmp_path, "boot_pes")
+    before = set(os.listdir("/tmp"))
+    env = dict(os.environ, NVSHMEM_HOST_BARRIER_TIMEOUT_S="60", TMPDIR="/tmp")
+    p = subprocess.Popen([exe, str(npes), str(tmp_path)], env=env, start_new_session=True)
+    try:
+        rc = p.wait(timeout=240)
+    except subprocess.TimeoutExpired:
+        os.killpg(p.pid, signal.SIGKILL)  # the group this test started: the app and its PE processes
+        p.wait()
+        raise
+    assert rc == 0, rc
+    check_exchange(tmp_path, npes, 4 << 20)
+    assert not [d for d in set(os.listdir("/tmp")) - before if d.startswith("nvshm-")]
