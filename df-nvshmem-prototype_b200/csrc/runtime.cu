@@ -511,8 +511,10 @@ int nvshmemx_init_bootstrap(const nvshmemx_bootstrap *bs, size_t heap_bytes_per_
     // on failure the empty name tells every rank to stop
   }
   std::vector<char> all((size_t)bs->size * kName);
-  if (bs->allgather(mine, all.data(), kName, bs->ctx) != 0)
+  if (bs->allgather(mine, all.data(), kName, bs->ctx) != 0) {
+    if (mine[0]) rmdir(mine);  // rank 0's directory, still empty
     return fail(NVSHMEMX_ERR_STATE, "nvshmemx_init_bootstrap: the allgather callback failed");
+  }
   const std::string dir(all.data(), strnlen(all.data(), kName - 1));
   if (dir.empty()) return fail(NVSHMEMX_ERR_STATE, "nvshmemx_init_bootstrap: rank 0 could not make a rendezvous directory");
   int rc = nvshmemx_init_process(bs->rank, bs->size, heap_bytes_per_pe, dir.c_str());

@@ -95,6 +95,30 @@ def test_bad_init_arguments_return_codes():
     assert r.stdout.split() == ["1", "1", "1"]
 
 
+def test_bootstrap_refusals_need_no_device(tmp_path):
+    """nvshmemx_init_bootstrap refuses a bad description, and a failing
+    allgather callback ends the start with ERR_STATE and leaves no
+    rendezvous directory behind (rank 0 made one before the callback)."""
+    code = PRE + "\n".join([
+        "import ctypes, os",
+        "lib.nvshmemx_set_error_mode(1)",
+        "AG = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)",
+        "class BS(ctypes.Structure):",
+        "    _fields_ = [('rank', ctypes.c_int), ('size', ctypes.c_int), ('allgather', AG), ('ctx', ctypes.c_void_p)]",
+        "fail = AG(lambda i, o, n, c: -1)",
+        "f = lib.nvshmemx_init_bootstrap",
+        "f.argtypes = [ctypes.c_void_p, ctypes.c_size_t]",
+        "bad = BS(2, 2, fail, None)",
+        "r1 = f(None, 1 << 20)",
+        "r2 = f(ctypes.byref(bad), 1 << 20)",
+        "r3 = f(ctypes.byref(BS(0, 1, fail, None)), 1 << 20)",
+        "print(r1, r2, r3, lib.nvshmemx_is_started(), len(os.listdir(os.environ['TMPDIR'])))",
+    ])
+    r = _run(code, env=dict(os.environ, TMPDIR=str(tmp_path)))
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.split() == ["1", "1", "4", "0", "0"]
+
+
 NATIVE = os.path.join(REPO, "tests", "native")
 
 
