@@ -5,7 +5,7 @@ and at the full 64-PE x 64 MiB size through per-PE checksums."""
 import numpy as np
 import pytest
 
-from nvshmem_b200 import (ERR_BOUNDS, MODE_THREAD, MODE_WARP, REQ_PUT,
+from nvshmem_b200 import (ERR_BOUNDS, ERR_NOMEM, MODE_THREAD, MODE_WARP, REQ_G, REQ_GET, REQ_PUT,
                           requests_bytes)
 from nvshmem_b200.traffic import c4_batch, check_disjoint
 from oracle.model import Model, checksum
@@ -106,6 +106,76 @@ def test_submit_end_to_end(shmem_factory):
         assert st == 0 and ms > 0
     om.apply_requests(reqs)
     assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+
+
+def expected_chunks(reqs, chunk):
+    """Work items of a batch: ceil(bytes / chunk) per PUT/GET, one per G,
+    SIGNAL and P."""
+    copies = np.isin(reqs["op"], (REQ_PUT, REQ_GET))
+    by = reqs["bytes"].astype(np.int64)
+    return int(((by[copies] + chunk - 1) // chunk).sum() + np.count_nonzero(~copies))
+
+
+@pytest.mark.parametrize("tma", [0, 3])
+def test_large_mixed_batch_and_small_table(shmem_factory, tma):
+    """6000 requests of mixed ops, widths and alignments (more than one plan
+    wave): the heaps match the oracle and the plan makes exactly one work
+    item per chunk; a bad request stops the batch, and so does a work-item
+    table too small for its chunks (nothing runs)."""
+    npes, heap = 8, 32 << 20
+    reqs = random_requests(78, 6000, npes, heap, max_bytes=40000)
+    assert len(reqs) >= 4096
+    chunk = 1024
+    cfg = dict(vec_bytes=16, chunk_bytes=chunk, unroll=4, threads=256, ctas_per_sm=2, grab=2,
+               tma_stages=tma, tma_stage_bytes=2048, tma_min_bytes=0)
+    sh, om = setup(shmem_factory, npes, heap)
+    payload = int(reqs["bytes"].sum()) + 8 * len(reqs)
+    with sh.batch(len(reqs), payload, 256) as b:
+        b.set_config(cfg)
+        b.upload(reqs)
+        b.execute(1)
+        assert b.stats()[0] == expected_chunks(reqs, chunk)
+        assert sh.status() == 0
+        om.apply_requests(reqs)
+        assert first_diff(heap_images(sh, npes, heap), om.heap) is None
+        before = heap_images(sh, npes, heap)
+        bad = reqs.copy()
+        bad[len(bad) // 2]["dst_pe"] = 99
+        b.upload(bad)
+        with pytest.raises(Exception) as ei:
+            b.execute(1)
+        assert ei.value.code == ERR_BOUNDS
+        sh.status()
+        assert np.array_equal(heap_images(sh, npes, heap), before)
+    # a table of len(reqs) + 1 items cannot hold the 1 KiB chunks
+    with sh.batch(len(reqs), 0, 256) as b:
+        b.set_config(cfg)
+        b.upload(reqs)
+        with pytest.raises(Exception) as ei:
+            b.execute(1)
+        assert ei.value.code == ERR_NOMEM
+    sh.status()
+    assert np.array_equal(heap_images(sh, npes, heap), before)
+
+
+def test_large_arena_offsets(shmem_factory):
+    """16 PEs x 1 GiB (a 16 GiB arena: work-item addresses far above 4 GiB
+    from the base). The batch leaves the same heaps as one call per
+    request."""
+    npes, heap = 16, 1 << 30
+    reqs = c4_batch(seed=51, n=20000, npes=npes, heap=heap, hi=64 << 10)
+    sh = shmem_factory(npes, heap)
+    with sh.batch(len(reqs), int(reqs["bytes"].sum()), 256) as b:
+        for pe in range(npes):
+            sh.fill_random(pe, 0, heap, 12)
+        b.upload(reqs)
+        b.execute(1)
+        batched = [sh.checksum(pe, 0, heap) for pe in range(npes)]
+        for pe in range(npes):
+            sh.fill_random(pe, 0, heap, 12)
+        b.percall(MODE_WARP, 1)
+        assert [sh.checksum(pe, 0, heap) for pe in range(npes)] == batched
+    assert sh.status() == 0
 
 
 def split_ends(n):
