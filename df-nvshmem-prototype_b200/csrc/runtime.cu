@@ -137,10 +137,13 @@ int publish_cfg() { return check_cuda(upload_cfg(rt().cfg), "cudaMemcpyToSymbol(
 // whole of what the prototype's offload barrier provides (its kernel
 // gathers the PEs' flags through PE 0, nvshmem_kernels.cu:56-102, because its
 // PEs are processes whose kernels run independently).  So here the barrier is
-// one small kernel on the default stream, launched normally: one CTA, whose
-// lanes write a BARRIER trace record for each PE when tracing is on.  (A
-// cooperative launch of one CTA per PE meeting on a ticket counter cost 3.6 to
-// 4.6 us per call, most of it the cooperative launch.)
+// an action on the legacy default stream: with tracing on, one small kernel
+// launched normally, one CTA whose lanes write a BARRIER trace record for
+// each PE; with tracing off, a wait on an event that has already completed
+// (cudaStreamWaitEvent is one of the actions that the legacy stream orders
+// against every blocking stream), which launches nothing.  (A cooperative
+// launch of one CTA per PE meeting on a ticket counter cost 3.6 to 4.6 us per
+// call, most of it the cooperative launch; the one-CTA kernel 2.6-4.1 us.)
 __global__ void offload_barrier_kernel(Cfg c, int npes) {
   if (!c.trace) return;
   const unsigned long long t = gtimer();
@@ -206,8 +209,14 @@ static size_t next_pow2(size_t x) {
   return p;
 }
 
+// Completed event that an untraced offload barrier waits on (see
+// nvshmem_barrier_all_offload); created at its first use after a start.
+static cudaEvent_t g_offload_ev = nullptr;
+
 static void release_all() {
   Runtime &r = rt();
+  if (g_offload_ev) cudaEventDestroy(g_offload_ev);
+  g_offload_ev = nullptr;
   if (r.d_trace) cudaFree(r.d_trace);
   if (r.d_trace_head) cudaFree(r.d_trace_head);
   r.d_trace = nullptr;
@@ -672,8 +681,23 @@ void nvshmem_barrier_all_offload(void) {
     if (rc) fail(rc, "nvshmem_barrier_all_offload: a PE thread left or the host barrier timed out");
     return;
   }
-  offload_barrier_kernel<<<1, 32, 0, 0>>>(r.cfg, r.npes);
-  check_cuda(cudaGetLastError(), "offload barrier launch");
+  // Every PE of this process runs on this GPU, so the legacy default stream
+  // already orders each PE's earlier work before its later work; an action on
+  // that stream also waits for all blocking streams and makes them wait for
+  // it.  Traced, the barrier is a one-CTA kernel that writes each PE's
+  // BARRIER record at its GPU time; untraced, it is a wait on a completed
+  // event, an action on the legacy stream that needs no kernel.
+  if (r.cfg.trace) {
+    offload_barrier_kernel<<<1, 32, 0, 0>>>(r.cfg, r.npes);
+    check_cuda(cudaGetLastError(), "offload barrier launch");
+    return;
+  }
+  if (!g_offload_ev) {
+    if (check_cuda(cudaEventCreateWithFlags(&g_offload_ev, cudaEventDisableTiming), "cudaEventCreate") ||
+        check_cuda(cudaEventRecord(g_offload_ev, 0), "cudaEventRecord"))
+      return;
+  }
+  check_cuda(cudaStreamWaitEvent(0, g_offload_ev, 0), "offload barrier");
 }
 
 // ---------------------------------------------------------- collective launch

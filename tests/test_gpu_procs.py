@@ -132,3 +132,17 @@ def test_bootstrap_from_the_applications_own_launcher(tmp_path, npes):
     assert rc == 0, rc
     check_exchange(tmp_path, npes, 4 << 20)
     assert not [d for d in set(os.listdir("/tmp")) - before if d.startswith("nvshm-")]
+
+
+def test_offload_barrier_orders_blocking_streams(tmp_path):
+    """nvshmem_barrier_all_offload is an action on the legacy default stream:
+    a kernel on a blocking stream after it runs only once the kernels that
+    blocking streams launched before it have finished
+    (tests/native/offload_order.cu). Without the barrier the same reader runs
+    beside the writer, which shows that the check can fail."""
+    exe = build(tmp_path, "offload_order")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr[-2000:])
+    counts = dict(kv.split("=") for kv in r.stdout.split() if "=" in kv)
+    assert int(counts["misses_with_barrier"]) == 0
+    assert int(counts["races_without"]) >= 1
