@@ -244,6 +244,14 @@ def run_extras(peak):
         ns, _ = sh.pingpong(flag, 0, 0, 10000, 20)
         out["pingpong_rtt_ns"] = {"p50": round(float(np.percentile(ns, 50)), 1),
                                   "p99": round(float(np.percentile(ns, 99)), 1), "iters": 10000}
+        # the same exchange with the flag word on 32 other 128-byte lines
+        # (other L2 slices): the round trip depends on where the line lives
+        p50s = []
+        for k in range(32):
+            off = (k * 37 * 4096 + k * 640) % (1 << 20) // 128 * 128
+            ns, _ = sh.pingpong(off, 2 << 20, 0, 3000, 20)
+            p50s.append(round(float(np.percentile(ns, 50)), 1))
+        out["pingpong_p50_ns_over_flag_lines"] = {"lines": 32, "iters": 3000, "sorted": sorted(p50s)}
     with Shmem(8, 1 << 20) as sh:
         bar = {}
         for ctas in (1, 16):

@@ -770,6 +770,10 @@ int nvshmemx_op_pingpong(size_t flag_off, size_t data_off, int len_elems, int it
   unsigned long long *gt = (unsigned long long *)(cyc + iters);
   int *data = (int *)(r.arena + data_off);
   int *flag = (int *)(r.arena + flag_off);
+  // both flag words start at 0, whatever an earlier exchange left there
+  for (int pe = 0; pe < 2; ++pe)
+    if ((rc = check_cuda(cudaMemsetAsync(r.arena + (size_t)pe * r.stride + flag_off, 0, 4, 0), "pingpong flags")))
+      return rc;
   void *args[] = {&data, &flag, &len_elems, &iters, &skip, &cyc, &gt};
   if ((rc = launch_collective((const void *)pingpong_kernel, dim3(1), dim3(32), args, 0, 0))) return rc;
   if ((rc = check_cuda(cudaDeviceSynchronize(), "pingpong"))) return rc;

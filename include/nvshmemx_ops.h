@@ -97,7 +97,8 @@ int nvshmemx_checksum(int pe, size_t off, size_t bytes, unsigned long long *out_
  * and echoes i+1 -- the put + flag exchange of
  * microbench/shmem_latency.cu:54-72; len_elems == 0 gives the flag-only
  * exchange of microbench/shmem_sync_latency.cu:54-70.  flag_off / data_off
- * are symmetric offsets and the flags must start at 0.  out_ns[iters]
+ * are symmetric offsets; both PEs' flag words are set to 0 first, so calls
+ * may reuse one flag.  out_ns[iters]
  * receives PE 0's per-iteration round trip in ns (may be NULL);
  * *out_total_ns the timed total. */
 int nvshmemx_op_pingpong(size_t flag_off, size_t data_off, int len_elems, int iters, int skip,

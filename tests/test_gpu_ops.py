@@ -41,6 +41,13 @@ def test_pingpong_flag_only_latency(shmem_factory):
     assert sh.read(1, flag, 4, np.int32)[0] == 10020
     p50 = float(np.median(ns))
     assert 0 < p50 < 50_000  # a round trip through L2, far below 50 us
+    # the flags are reset by the call: a second exchange on the same words
+    # still waits for every echo (it would run far faster if the waits passed
+    # on the values the first one left)
+    ns2, _ = sh.pingpong(flag, 0, 0, 10000, 20)
+    assert sh.status() == 0
+    assert 0.5 * p50 < float(np.median(ns2)) < 2 * p50
+    assert sh.read(1, flag, 4, np.int32)[0] == 10020
 
 
 @pytest.mark.parametrize("counted", [False, True])
