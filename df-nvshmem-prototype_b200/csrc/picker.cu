@@ -16,6 +16,7 @@
 // contents, so the choice only changes the time.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdint.h>
 #include <string.h>
 
 #include <algorithm>
@@ -235,12 +236,12 @@ extern "C" int nvshmemx_batch_execute_picked(nvshmemx_batch *b, nvshmemx_picker 
       g->width = width;
       g->align = align;
     } else {
-      key = 0xffffffffu;  // SIGNAL, P, G
+      key = 0xffffffffu;  // SIGNAL, P, G: one element each (their `bytes` field is not used)
       g = &by_key[key];
       g->scalar = 1;
     }
     g->idx.push_back(i);
-    g->bytes += q.bytes;
+    g->bytes += g->scalar ? (q.op != NVSHMEMX_REQ_SIGNAL && q.dtype == NVSHMEMX_DT_DOUBLE ? 8 : 4) : q.bytes;
   }
   std::vector<Group> gs;
   gs.reserve(by_key.size());
@@ -282,7 +283,9 @@ extern "C" int nvshmemx_batch_execute_picked(nvshmemx_batch *b, nvshmemx_picker 
   // requests already sit in that buffer, they are gathered through a
   // temporary array first.
   nvshmemx_request *pinned = nvshmemx_batch_host_buffer(b);
-  const bool aliased = reqs < pinned + batch_capacity(b) && pinned < reqs + n;
+  const uintptr_t pin0 = reinterpret_cast<uintptr_t>(pinned), req0 = reinterpret_cast<uintptr_t>(reqs);
+  const bool aliased = req0 < pin0 + (size_t)batch_capacity(b) * sizeof(nvshmemx_request) &&
+                       pin0 < req0 + (size_t)n * sizeof(nvshmemx_request);
   std::vector<nvshmemx_request> tmp;
   nvshmemx_request *perm = pinned;
   if (aliased) {
@@ -348,7 +351,13 @@ extern "C" int nvshmemx_batch_execute_picked(nvshmemx_batch *b, nvshmemx_picker 
     }
   if (!rc) rc = check_cuda(cudaEventRecord(p->ev_t[2], st), "cudaEventRecord");
   if (!rc) rc = check_cuda(cudaStreamSynchronize(st), "batch_execute_picked");
-  if (rc) return rc;
+  if (rc) {
+    // let whatever was enqueued finish before the caller reuses the buffers
+    for (int m = 0; m < 4; ++m)
+      if (used[m]) cudaStreamSynchronize(p->aux[m]);
+    cudaStreamSynchronize(st);
+    return rc;
+  }
   float ms = 0, run_ms = 0;
   cudaEventElapsedTime(&ms, p->ev_t[0], p->ev_t[2]);
   cudaEventElapsedTime(&run_ms, p->ev_t[1], p->ev_t[2]);
