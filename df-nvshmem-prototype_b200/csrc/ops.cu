@@ -993,6 +993,7 @@ int nvshmemx_op_strided_read(size_t off, size_t set_off, int nsets, size_t rows,
   size_t span = 0, last = 0;
   if (nsets < 1 || ctas_per_pe < 1 || iters < 1 || rows < 1 || stride < 8 || (off | set_off | stride) % 8 ||
       !mul_ok(rows - 1, stride, &span) || !mul_ok((size_t)(nsets - 1), set_off, &last) ||
+      span > r.heap_bytes ||  // so that span + 8 cannot wrap
       !range_ok(last, span + 8, r.heap_bytes) || !range_ok(off, last + span + 8, r.heap_bytes))
     return fail(NVSHMEMX_ERR_INVALID, "strided_read: bad arguments or elements outside the heap");
   unsigned long long *sink = (unsigned long long *)g_out_buf.get(64);

@@ -233,6 +233,12 @@ def test_host_checks_reject_wrapping_arguments(shmem_factory):
     with pytest.raises(Exception) as ei:
         sh.wait_test(huge, 1, 1000)
     assert ei.value.code == ERR_INVALID
+    with pytest.raises(Exception) as ei:  # (rows - 1) * stride + 8 wraps to 0
+        sh.strided_read(0, 8, 1, (1 << 61), 8, 1, 1)
+    assert ei.value.code == ERR_INVALID
+    with pytest.raises(Exception) as ei:  # one row past the heap
+        sh.strided_read(0, 8, 1, (1 << 20) // 8 + 1, 8, 1, 1)
+    assert ei.value.code == ERR_INVALID
     # the status word reports the first host-side refusal once, and no device
     # error: nothing was launched
     assert sh.status() == ERR_INVALID
@@ -241,6 +247,17 @@ def test_host_checks_reject_wrapping_arguments(shmem_factory):
     with pytest.raises(Exception) as ei:
         sh2.pingpong(huge, 0, 0, 1)
     assert ei.value.code == ERR_INVALID
+
+
+def test_strided_read_reads_the_rows_it_is_given(shmem_factory):
+    """nvshmemx_op_strided_read (the halo's x-face read ceiling): a valid
+    call over the last row of the heap runs and leaves the status clean."""
+    heap = 1 << 20
+    sh = shmem_factory(8, heap)
+    n = 64
+    ms = sh.strided_read(0, (n - 1) * 8, 2, heap // (8 * n), 8 * n, 4, 3)
+    assert ms > 0
+    assert sh.status() == 0
 
 
 def test_wait_timeout_reports_and_returns(shmem_factory):
