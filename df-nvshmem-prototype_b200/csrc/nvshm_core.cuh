@@ -200,9 +200,10 @@ __device__ __forceinline__ void copy_body(char *__restrict__ dst, const char *__
       V v[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) v[u] = s[i + (unsigned long long)u * nthr];
-      // between this round's loads and its stores: the stores of one round
-      // and the loads of the next stay free to interleave (measured: placed
-      // before the loads, the prefetch cost 15-23% on copies already in L2)
+      // between this iteration's loads and its stores: the stores of one
+      // iteration and the loads of the next stay free to interleave
+      // (measured: placed before the loads, the prefetch cost 15-23% on
+      // copies already in L2)
       if (pf_on) {
         uintptr_t want = ((uintptr_t)(s + i) + dist) & ~(uintptr_t)15;
         if (want > pf_end) want = pf_end;
