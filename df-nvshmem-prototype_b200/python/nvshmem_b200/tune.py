@@ -75,6 +75,8 @@ def robust_choice(sh, spec: dict, top: list[dict], seeds, reps: int = 5, rounds:
                 for i, r in enumerate(rows):
                     ms[i].append(r["ms_median"] if r["status"] == 0 and r["ms_median"] > 0 else float("inf"))
         per_seed[seed] = [statistics.median(v) for v in ms]
+        if min(per_seed[seed]) == float("inf"):
+            raise RuntimeError(f"robust_choice: no configuration ran on the seed-{seed} batch")
     ratios = []
     for i in range(len(cands)):
         rs = [per_seed[s][i] / min(per_seed[s]) for s in seeds]

@@ -73,3 +73,17 @@ def test_committed_table_is_consistent():
     assert ranked[0]["cfg"] == rob["chosen"] == t["best"]
     # the candidates are the sweep's leading configurations
     assert [c["cfg"] for c in rob["candidates"]] == cfgs[:len(rob["candidates"])]
+
+
+def test_robust_choice_refuses_a_batch_where_nothing_ran(monkeypatch):
+    from nvshmem_b200 import tune
+
+    def failing(b, cands=None, reps=5, flush_bytes=0):
+        rows = [dict(cfg=c.as_dict(), ms_median=-1.0, ms_min=-1.0, exec_ms_median=-1.0, status=1) for c in cands]
+        return rows, rows[0]
+
+    monkeypatch.setattr(tune, "tune_batch", failing)
+    base = dict(vec_bytes=16, chunk_bytes=16384, unroll=4, threads=128, ctas_per_sm=0, grab=2, tma_stages=2,
+                tma_stage_bytes=8192, tma_min_bytes=512, stream=0, stream_planners=2)
+    with pytest.raises(RuntimeError):
+        tune.robust_choice(_FakeShmem([4]), dict(seed=4, n=100, npes=4, heap=1 << 20), [base], [4], reps=1, rounds=1)
