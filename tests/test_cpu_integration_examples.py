@@ -44,3 +44,19 @@ def test_python_examples_parse():
     assert blocks
     for k, code in enumerate(blocks):
         compile(code, f"INTEGRATION.md python block {k}", "exec")
+
+
+def test_cgo_example_uses_declared_names():
+    """Go is not installed here: check instead that every C.name the cgo
+    example calls or names is declared in the headers it includes."""
+    blocks = _blocks("go")
+    assert blocks
+    names = set(re.findall(r"\bC\.([A-Za-z_][A-Za-z0-9_]*)", "".join(blocks)))
+    builtin = {"int", "float", "GoString", "char", "size_t", "longlong", "ulonglong"}
+    headers = ""
+    for h in ("nvshmem.h", "nvshmemx.h", "nvshmemx_batch.h"):
+        with open(os.path.join(REPO, "include", h)) as f:
+            headers += f.read()
+    missing = [n for n in sorted(names - builtin) if not re.search(r"\b" + n + r"\b", headers)]
+    assert not missing, missing
+    assert "nvshmemx_batch_submit" in names and "nvshmemx_last_error_string" in names
