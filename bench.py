@@ -210,7 +210,13 @@ def startup_tune(b, k=4, reps=7):
     with open(TUNED) as f:
         table = json.load(f)
     if "robust" in table:
-        rows = sorted(table["robust"]["candidates"], key=lambda r: (r["worst_ratio"], r["mean_ratio"]))[:k]
+        ranked = sorted(table["robust"]["candidates"], key=lambda r: (r["worst_ratio"], r["mean_ratio"]))
+        rows = ranked[:k]
+        # keep an 8-warp shape among them: the 4-warp shapes have a slow mode
+        # on some boxes that the 8-warp ones do not share
+        wide = [r for r in ranked if r["cfg"]["threads"] >= 256]
+        if wide and not any(r["cfg"]["threads"] >= 256 for r in rows):
+            rows[-1] = wide[0]
     else:
         rows = [r for r in table["results"] if r.get("ms_median", -1) > 0 and not r["cfg"].get("stream", 0)][:k]
     cands = []

@@ -72,7 +72,7 @@ int nvshmemx_tune_candidates(nvshmemx_batch_config *out, int max, int min_chunk_
     for (int sb : {4096, 8192, 16384})
       for (int t : {128, 256})
         for (int ch : {16384, 65536})
-          for (int mb : {512, 2048}) {
+          for (int mb : {512, 1024, 2048}) {
             c.vec_bytes = 16;
             c.unroll = 4;
             c.chunk_bytes = ch;

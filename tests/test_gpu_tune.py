@@ -37,5 +37,6 @@ def test_tuner_ranks_and_keeps_results_exact(shmem_factory):
 
 def test_candidate_grid():
     c = tune.candidates(min_chunk=256)
-    assert len(c) == 112 and sum(1 for x in c if x.tma_stages) == 58 and sum(x.stream for x in c) == 6
+    assert len(c) == 138 and sum(1 for x in c if x.tma_stages) == 84 and sum(x.stream for x in c) == 6
+    assert sorted({x.tma_min_bytes for x in c if x.tma_stages and not x.stream}) == [512, 1024, 2048]
     assert all(x.chunk_bytes >= 4096 for x in tune.candidates(min_chunk=4096))
