@@ -195,10 +195,26 @@ def l2_flusher():
     return flush
 
 
+def startup_rows(table, k=4):
+    """The k table rows the startup tune re-times: the k most robust
+    graph-mode shapes (smallest worst slowdown over the tuner's C4 seeds),
+    with the best 8-warp shape in place of the last when none of them has 8
+    warps (the 4-warp shapes have a slow mode on some boxes that the 8-warp
+    ones do not share); the sweep's first k for a table without that
+    ranking."""
+    if "robust" in table:
+        ranked = sorted(table["robust"]["candidates"], key=lambda r: (r["worst_ratio"], r["mean_ratio"]))
+        rows = ranked[:k]
+        wide = [r for r in ranked if r["cfg"]["threads"] >= 256]
+        if wide and not any(r["cfg"]["threads"] >= 256 for r in rows):
+            rows[-1] = wide[0]
+        return rows
+    return [r for r in table["results"] if r.get("ms_median", -1) > 0 and not r["cfg"].get("stream", 0)][:k]
+
+
 def startup_tune(b, k=4, reps=7):
-    """The tuned table's k best graph-mode configurations (ranked by their
-    worst slowdown over the tuner's C4 seeds when the table holds that
-    ranking, else by the sweep), re-timed on this box by the library's autotuner
+    """The tuned table's k best graph-mode configurations (startup_rows),
+    re-timed on this box by the library's autotuner
     (nvshmemx_tune_batch: L2 flushed before every run, median of `reps`),
     which leaves the fastest set on the batch.  Done before the warm-up
     steps, outside every timed region: the ranking of the leading shapes
@@ -209,16 +225,7 @@ def startup_tune(b, k=4, reps=7):
         return None
     with open(TUNED) as f:
         table = json.load(f)
-    if "robust" in table:
-        ranked = sorted(table["robust"]["candidates"], key=lambda r: (r["worst_ratio"], r["mean_ratio"]))
-        rows = ranked[:k]
-        # keep an 8-warp shape among them: the 4-warp shapes have a slow mode
-        # on some boxes that the 8-warp ones do not share
-        wide = [r for r in ranked if r["cfg"]["threads"] >= 256]
-        if wide and not any(r["cfg"]["threads"] >= 256 for r in rows):
-            rows[-1] = wide[0]
-    else:
-        rows = [r for r in table["results"] if r.get("ms_median", -1) > 0 and not r["cfg"].get("stream", 0)][:k]
+    rows = startup_rows(table, k)
     cands = []
     for r in rows:
         c = L.BatchConfig()

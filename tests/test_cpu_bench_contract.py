@@ -51,3 +51,23 @@ def test_c3_full_size_check_matches_the_oracle():
             want = np.ascontiguousarray(bench.c3_faces(blocks[bench.c3_nbr(q, g)], n)[g ^ 1]).view(np.uint8).reshape(-1)
             assert np.array_equal(got[g * n * n * 8:(g + 1) * n * n * 8], want), (q, g)
         assert np.array_equal(om.heap[q, block + ghosts:block + ghosts + 24].view(np.int32), np.full(6, 4, np.int32))
+
+
+def test_startup_rows_keep_an_eight_warp_shape():
+    """The startup tune re-times the most robust shapes of the tuned table
+    and always keeps an 8-warp one among them."""
+    sys.path.insert(0, REPO)
+    import bench
+
+    def row(threads, worst, mb=512):
+        return {"cfg": {"threads": threads, "tma_min_bytes": mb}, "worst_ratio": worst, "mean_ratio": worst}
+
+    table = {"robust": {"candidates": [row(128, 1.00), row(128, 1.01, 1024), row(128, 1.02), row(128, 1.03, 2048),
+                                       row(256, 1.05), row(256, 1.04, 1024)]}}
+    rows = bench.startup_rows(table, 4)
+    assert [r["cfg"]["threads"] for r in rows] == [128, 128, 128, 256]
+    assert rows[-1]["worst_ratio"] == 1.04  # the best-ranked 8-warp shape
+    assert rows[0]["worst_ratio"] == 1.00
+    with open(bench.TUNED) as f:
+        committed = bench.startup_rows(json.load(f), 4)
+    assert len(committed) == 4 and any(r["cfg"]["threads"] >= 256 for r in committed)
