@@ -71,3 +71,23 @@ def test_startup_rows_keep_an_eight_warp_shape():
     with open(bench.TUNED) as f:
         committed = bench.startup_rows(json.load(f), 4)
     assert len(committed) == 4 and any(r["cfg"]["threads"] >= 256 for r in committed)
+
+
+def test_reference_arm_under_torchrun_prints_one_line():
+    """Launched as the driver launches N > 1 (torchrun, 2 ranks here, on the
+    host cores): rank 0 alone runs and prints one line, the other rank exits
+    0 without work."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    env = dict(os.environ, NVSHMEM_B200_LIB=os.path.join(REPO, "no-such-library.so"))
+    r = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+                        "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(REPO, "bench.py"),
+                        "--impl", "reference", "--gpus", "2", "--steps", "2", "--warmup", "3"],
+                       capture_output=True, text=True, timeout=600, cwd=REPO, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["steps"] == 2
